@@ -1,0 +1,118 @@
+"""CPU: pin the oracle against the reference's golden vectors and against the reference itself.
+
+* FFT building blocks vs the reference's CoreFFT known-answer vectors (digests in golden/fft_kat.json).
+* Whole fixed-point frames vs the reference emulator's CRC (golden/fixed_frames.json, produced by
+  golden/make_golden.py running ``silicon_emulator.form_image`` unmodified).
+* Float frames vs the reference ``pfa()`` digests (golden/float_frames.json).
+* Where the reference checkout is present: stage-by-stage equality with the reference functions.
+"""
+import json
+import zlib
+
+import numpy as np
+import pytest
+
+from oracle import fft_kat, fixed_emulator as fe, float_pfa as fp
+from pfa_b200 import synth, geometry
+
+
+def _crc(a):
+    return zlib.crc32(np.ascontiguousarray(a).tobytes()) & 0xFFFFFFFF
+
+
+def test_fft_kat_vectors(golden_dir):
+    g = json.loads((golden_dir / "fft_kat.json").read_text())
+    for name, x in fft_kat.stimuli(g["n"]).items():
+        c = g["cases"][name]
+        lsb, e_in = fft_kat.block_exp(x, g["nbits"])
+        ir, ii = fft_kat.codes(x, lsb)
+        assert _crc(np.stack([ir, ii], 1).astype("<i2")) == c["in_crc"], name
+        y, ex = fft_kat.fft_bfp_line(x, g["nbits"], g["nbits_tw"])
+        orr, oi = fft_kat.codes(y, 2.0 ** ex[-1], exact=True)
+        assert _crc(np.stack([orr, oi], 1).astype("<i2")) == c["out_crc"], name
+        assert ex == c["stage_exps"], name
+
+
+FIXED = json.loads((__import__("pathlib").Path(__file__).parent / "golden" / "fixed_frames.json").read_text())["cases"]
+
+
+@pytest.mark.parametrize("name", sorted(FIXED))
+def test_fixed_oracle_matches_reference_crc(name):
+    c = FIXED[name]
+    sc = synth.make_scene(**c["scene"])
+    if _crc(sc.signal) != c["input_crc"]:
+        pytest.skip("synthetic input not bit-identical on this host")
+    tb = geometry.prepare_tables_from_scene(sc)
+    img, _ = fe.form_image(sc.signal, tb, c["grid"], c["range_sinc"], c["az_sinc"])
+    assert fe.frame_crc(img) == c["image_crc"]
+
+
+FLOAT = json.loads((__import__("pathlib").Path(__file__).parent / "golden" / "float_frames.json").read_text())["cases"]
+
+
+@pytest.mark.parametrize("name", sorted(FLOAT))
+def test_float_oracle_matches_reference(name):
+    c = FLOAT[name]
+    sc = synth.make_scene(**c["scene"])
+    if _crc(sc.signal) != c["input_crc"]:
+        pytest.skip("synthetic input not bit-identical on this host")
+    tb = geometry.prepare_tables_from_scene(sc)
+    det = fp.detect(fp.pfa_image(sc.signal, tb["freq"], tb["ax"], tb["ay"], tb["sgn"]))
+    assert _crc(det) == c["detect_crc"]
+
+
+def test_sinc_table_matches_reference(ref_modules):
+    ref = np.asarray(ref_modules.grv.sinc_table_q15(256, 32), np.int64)
+    assert np.array_equal(fe.sinc_table_q15(), ref)
+
+
+def test_stages_match_reference(ref_modules):
+    """Each restated stage equals the reference function on the same operands."""
+    emu, ser, fx = ref_modules.emu, ref_modules.ser, ref_modules.fx
+    rng = np.random.default_rng(5)
+    # bracket + Q15 weight, ascending and descending source axes, out-of-span queries included
+    for asc in (True, False):
+        xp = np.sort(rng.uniform(-3, 3, 300))
+        xp = xp if asc else xp[::-1]
+        q = rng.uniform(-3.5, 3.5, 700)
+        i0, w0 = ser.interp_coeffs(q, xp)
+        i1, w1 = fe.bracket_q15(q, xp)
+        assert np.array_equal(i0, i1) and np.array_equal(w0, w1)
+    # sinc / lerp gathers on adversarial int16 extremes
+    sn = 96
+    src = rng.choice([-32768, 32767, -1, 0, 1, 12345, -23456], size=sn) + 1j * rng.choice(
+        [-32768, 32767, -1, 0, 1, 777, -999], size=sn)
+    idx = rng.integers(-1, sn - 1, 500).astype(np.int32)
+    wq = rng.integers(0, 32768, 500).astype(np.int16)
+    wq[idx < 0] = 0
+    r0 = emu.apply_sinc(src, idx, wq, sn)
+    rr, ri = fe.gather_sinc(src.real.astype(np.int64), src.imag.astype(np.int64), idx.astype(np.int64),
+                            wq.astype(np.int64), sn)
+    assert np.array_equal(r0.real, rr) and np.array_equal(r0.imag, ri)
+    r0 = emu.apply_fixed(src.astype(np.complex64), idx, wq)
+    rr, ri = fe.gather_lerp(src.real.astype(np.int64), src.imag.astype(np.int64), idx.astype(np.int64),
+                            wq.astype(np.int64), f32_product=True)
+    assert np.array_equal(r0.real, rr) and np.array_equal(r0.imag, ri)
+    # window with odd lengths (the 32768 centre tap wraps to -32768)
+    g = rng.integers(-32768, 32768, (64, 64)) + 1j * rng.integers(-32768, 32768, (64, 64))
+    w0 = emu.window_fixed(g, 63, 61)
+    wr, wi = fe.window_q15(g.real.astype(np.int64), g.imag.astype(np.int64), 63, 61)
+    assert np.array_equal(w0.real, wr) and np.array_equal(w0.imag, wi)
+    # BFP FFT pass
+    x = rng.integers(-32768, 32768, (16, 256)) + 1j * rng.integers(-32768, 32768, (16, 256))
+    y0, e0 = emu.fft_pass_bfp(x.astype(np.complex128))
+    yr, yi, e1 = fe.fft_pass(x.real.astype(np.int64), x.imag.astype(np.int64))
+    assert np.array_equal(y0.real, yr) and np.array_equal(y0.imag, yi) and np.array_equal(e0, e1)
+    # detect
+    z = x[:, :64]
+    assert np.array_equal(emu.detect_fixed(z), fe.detect_q(z.real.astype(np.int64), z.imag.astype(np.int64)))
+
+
+def test_prepare_tables_matches_reference(ref_modules):
+    sc = synth.make_scene(300, 280, n_targets=4, seed=3, jitter=0.4)
+    from oracle import refshim
+    t0 = refshim.reference_tables(sc)
+    t1 = geometry.prepare_tables_from_scene(sc)
+    for k in ("ax", "ay", "freq", "KR", "KC", "tan_phi", "window"):
+        assert np.array_equal(np.asarray(t0[k]), np.asarray(t1[k])), k
+    assert t0["sgn"] == t1["sgn"] and tuple(t0["dims"]) == tuple(t1["dims"])
