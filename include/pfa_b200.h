@@ -1,0 +1,154 @@
+/*
+ * pfa_b200.h -- C ABI of the B200 Polar Format Algorithm (PFA) focusing engine.
+ *
+ * The engine replaces the focusing datapath of the reference SAR image former:
+ *
+ *   fixed point  -> the body of silicon_emulator.form_image() after the CPHD read
+ *                   (mpfs/host/silicon_emulator.py:226-249): Q0 int16 quantise, resample_fixed
+ *                   (:125-156), window_fixed (:165-195), fft_pass_bfp x2 with corner turns
+ *                   (:198-205, :241-247), detect_fixed (:208-213).  Bit-exact: same uint16 image,
+ *                   same CRC-32.
+ *   float        -> form_image_pfa.resample_kspace + focus + |.| (src/form_image_pfa.py:165-246,
+ *                   mpfs/host/accel.py:39-44), i.e. AccelBackend.focus(signal, tables).
+ *
+ * It stands where the board ABI sar_form_image(spin_limit) -> sar_seq_status_t stands
+ * (mpfs/fpga/libero_sar/softconsole/mpfs-hal-ddr-demo/src/sar/sar_sequencer.c:1432, status enum
+ * sar_sequencer.h:19-27): the job vectors below are the board's staged job (the 10-role DDR format of
+ * mpfs/host/serialize_inputs.py:1-30, with the emulator's floor tapers), and every call returns a
+ * status code instead of raising.
+ *
+ * Conventions: plain pointers and sizes; "dev" pointers are CUDA device pointers, "host" pointers are
+ * host memory; `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).  Calls on one
+ * plan are not thread-safe; distinct plans are independent.  All launches are stream-ordered and
+ * asynchronous unless the name ends in _host.
+ */
+#ifndef PFA_B200_H
+#define PFA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes, modelled on sar_seq_status_t (sar_sequencer.h:19-27). */
+typedef enum pfa_status {
+    PFA_OK = 0,
+    PFA_ERR_BAD_CONFIG = 1,   /* unsupported mode/grid/interp combination                       */
+    PFA_ERR_BAD_DIMS = 2,     /* grid smaller than the scene (standalone_emulator_README.md:90-95) */
+    PFA_ERR_BAD_ARG = 3,      /* NULL or misaligned pointer, bad size                            */
+    PFA_ERR_NOT_READY = 4,    /* job vectors not set before a form call                          */
+    PFA_ERR_CUDA = 5,         /* CUDA runtime error (message in pfa_last_error)                  */
+    PFA_ERR_ALLOC = 6,        /* device allocation failed                                        */
+    PFA_ERR_TIMEOUT = 7,      /* a bounded wait ran out                                          */
+    PFA_ERR_NO_DEVICE = 8     /* no usable sm_100 device                                         */
+} pfa_status;
+
+enum pfa_mode { PFA_MODE_FIXED = 0, PFA_MODE_FLOAT32 = 1, PFA_MODE_MIXED = 2 };
+enum pfa_interp { PFA_INTERP_LERP = 0, PFA_INTERP_SINC = 1 };
+
+/* Output layout of the float path. */
+enum pfa_layout {
+    PFA_LAYOUT_CENTRED = 0,   /* fftshift(fft2(ifftshift(pad))): (m2 rows = cross, n2 cols = range), form_image_pfa */
+    PFA_LAYOUT_NATURAL = 1    /* fft2(pad) without shifts                                            */
+};
+
+/* What the float path writes. */
+enum pfa_detect {
+    PFA_DETECT_MAG = 0,       /* float32 |z|   (accel.NumpyBackend.focus)  */
+    PFA_DETECT_POWER = 1,     /* float32 |z|^2                            */
+    PFA_DETECT_COMPLEX = 2    /* complex64 z                              */
+};
+
+typedef struct pfa_config {
+    int32_t mode;          /* pfa_mode                                                      */
+    int32_t m;             /* pulses after decimation                                       */
+    int32_t n;             /* samples per pulse after decimation                            */
+    int32_t grid;          /* fixed: square output grid G (pow2, 64..16384, >= m and n)      */
+                           /* float: 0 = pow2(m) x pow2(n) as form_image_pfa.focus           */
+    int32_t range_interp;  /* pfa_interp for pass 1 (--range-sinc)                          */
+    int32_t az_interp;     /* pfa_interp for pass 2 (--az-sinc)                             */
+    int32_t device;        /* CUDA device ordinal                                           */
+    int32_t reserved[9];
+} pfa_config;
+
+/* Fixed-point job: host pointers, copied at pfa_set_fixed_job.  Built exactly as
+ * silicon_emulator.resample_fixed/window_fixed build them (silicon_emulator.py:131-141, 185-188). */
+typedef struct pfa_fixed_job {
+    const float *f0;          /* [m]   freq[:,0] as float32                                     */
+    const float *df;          /* [m]   (freq[:,1]-freq[:,0]) as float32                          */
+    const float *pr;          /* [m]   radial projection as float32                              */
+    const float *tan_s;       /* [m]   tan(phi) sorted ascending, float32                        */
+    const int32_t *inv_order; /* [m]   pass-1 destination slot of pulse i (argsort(argsort(tan_phi))) */
+    const float *kr_grid;     /* [G]   KR padded with the out-of-span sentinel                   */
+    const float *kc_grid;     /* [G]   KC padded with the out-of-span sentinel                   */
+    const int32_t *ham_r;     /* [G]   floor(hamming(n)*32768), zero pad; NULL = built in        */
+    const int32_t *ham_c;     /* [G]   floor(hamming(m)*32768), zero pad; NULL = built in        */
+    const int16_t *twiddle;   /* [G/2][2] floor(exp(-2pi j k/G)*32768) clipped; NULL = built in  */
+    const int16_t *sinc_q15;  /* [256][32] polyphase table; NULL = built in                     */
+} pfa_fixed_job;
+
+/* Float job: host pointers, copied at pfa_set_float_job.  Mirrors form_image_pfa.resample_kspace
+ * (src/form_image_pfa.py:177-217); freq[i,k] = f0[i] + k*df[i]. */
+typedef struct pfa_float_job {
+    const double *f0;         /* [m] */
+    const double *df;         /* [m] */
+    const double *pr;         /* [m] radial projection                                          */
+    const double *tan_s;      /* [m] tan(phi) sorted ascending                                   */
+    const int32_t *order;     /* [m] argsort(tan_phi)                                            */
+    const double *kr_grid;    /* [n] KR                                                          */
+    const double *kc_grid;    /* [m] KC                                                          */
+    const double *ham_m;      /* [m] hamming(m); NULL = no window                               */
+    const double *ham_n;      /* [n] hamming(n); NULL = no window                               */
+    int32_t sgn;              /* CPHD SGN: -1 forward FFT, +1 inverse (with 1/(m2 n2))            */
+    int32_t layout;           /* pfa_layout                                                      */
+} pfa_float_job;
+
+typedef struct pfa_plan pfa_plan;
+
+/* Plan lifetime.  Allocates the device workspace for one frame of the configured shape.
+ * Replaces: allocation of the emulator's (grid x grid) intermediates (silicon_emulator.py:153, 233-247). */
+pfa_status pfa_plan_create(const pfa_config *cfg, pfa_plan **out);
+pfa_status pfa_plan_destroy(pfa_plan *plan);
+/* Device bytes held by the plan's workspace. */
+size_t pfa_plan_workspace_bytes(const pfa_plan *plan);
+
+/* Job upload.  Replaces: the geometry block of resample_fixed (silicon_emulator.py:131-141) and the
+ * taper build of window_fixed (:185-188) / serialize_inputs.serialize (:206-225). */
+pfa_status pfa_set_fixed_job(pfa_plan *plan, const pfa_fixed_job *job);
+/* Replaces: the geometry block of form_image_pfa.resample_kspace (src/form_image_pfa.py:177-211). */
+pfa_status pfa_set_float_job(pfa_plan *plan, const pfa_float_job *job);
+
+/* Fixed-point frame from the complex64 phase history (m x n, interleaved re/im float32, device).
+ * Replaces: silicon_emulator.form_image lines :226-249 (Q0 quantise .. detect_fixed).
+ * img_dev: uint16 [G][G], rows = range bins, cols = cross bins (the emulator's natural order). */
+pfa_status pfa_form_fixed(pfa_plan *plan, const float *sig_dev, uint16_t *img_dev, void *stream);
+/* Same, from an already quantised int16 I/Q signal (m x n x 2, device): the board's sig.bin
+ * (serialize_inputs.py:1-30, ddr_layout.quantize_iq16).  Replaces :233-249. */
+pfa_status pfa_form_fixed_iq16(pfa_plan *plan, const int16_t *sig_iq_dev, uint16_t *img_dev, void *stream);
+/* End-to-end host variant: copies the host signal in, forms, copies the image out, synchronises. */
+pfa_status pfa_form_fixed_host(pfa_plan *plan, const float *sig_host, uint16_t *img_host);
+
+/* Per-row BFP exponents of the last fixed frame (silicon_emulator.fft_pass_bfp's `e`, :198-205):
+ * e_range[n] (FFT-1 rows = range bins < n; rows >= n are all-zero and have exponent 0),
+ * e_az[G] (FFT-2 rows = cross bins), q0_exp = the Q0 block exponent.  Host pointers; synchronises. */
+pfa_status pfa_get_fixed_exponents(pfa_plan *plan, int32_t *e_range, int32_t *e_az, int32_t *q0_exp);
+
+/* Float frame from the complex64 phase history (device).  out_dev: float32 [m2][n2] for
+ * PFA_DETECT_MAG/POWER, complex64 [m2][n2] for PFA_DETECT_COMPLEX.
+ * Replaces: accel.NumpyBackend.focus (mpfs/host/accel.py:39-44) / form_image_pfa.pfa (:243-246). */
+pfa_status pfa_form_float(pfa_plan *plan, const float *sig_dev, void *out_dev, int32_t detect, void *stream);
+pfa_status pfa_form_float_host(pfa_plan *plan, const float *sig_host, void *out_host, int32_t detect);
+
+/* Diagnostics. */
+const char *pfa_status_string(pfa_status st);
+pfa_status pfa_last_error(const pfa_plan *plan, char *buf, size_t len);
+/* Library version string. */
+const char *pfa_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PFA_B200_H */

@@ -1,0 +1,327 @@
+// C ABI of the PFA engine: plan lifecycle, job upload, frame entry points, diagnostics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "pfa_internal.h"
+
+namespace pfa {
+#include "gen/sinc_q15.inc"   // kSincQ15[256 * 32], generated at build time by the exact-rational recipe
+
+void build_sinc_table(int16_t *tab) { std::memcpy(tab, kSincQ15, sizeof(kSincQ15)); }
+
+void build_twiddles_q15(int G, int16_t *tw2) {
+    // floor(exp(-2 pi j k / G) * 32768) clipped to int16 (src/fixedpoint.py:277, quant mode 'trunc')
+    for (int k = 0; k < G / 2; ++k) {
+        const double th = (-2.0 * M_PI * (double)k) / (double)G;
+        const double c = std::floor(std::cos(th) / std::ldexp(1.0, -15));
+        const double s = std::floor(std::sin(th) / std::ldexp(1.0, -15));
+        tw2[2 * k] = (int16_t)std::min(std::max(c, -32768.0), 32767.0);
+        tw2[2 * k + 1] = (int16_t)std::min(std::max(s, -32768.0), 32767.0);
+    }
+}
+
+void build_hamming_q15(int len, int size, int32_t *out) {
+    for (int i = 0; i < size; ++i) out[i] = 0;
+    if (len == 1) { out[0] = 32768; return; }
+    for (int i = 0; i < len; ++i) {
+        const double h = 0.54 + 0.46 * std::cos(M_PI * (double)(2 * i + 1 - len) / (double)(len - 1));
+        out[i] = (int32_t)std::floor(h * 32768.0);
+    }
+}
+}  // namespace pfa
+
+namespace {
+
+bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+int ilog2(int v) { int l = 0; while ((1 << l) < v) ++l; return l; }
+
+pfa_status fail(pfa_plan *p, pfa_status st, const std::string &msg) {
+    if (p) p->err = msg;
+    return st;
+}
+
+pfa_status cuda_fail(pfa_plan *p, cudaError_t e, const char *where) {
+    if (p) p->err = std::string(where) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? PFA_ERR_ALLOC : PFA_ERR_CUDA;
+}
+
+template <class T>
+cudaError_t dalloc(T **ptr, size_t count, size_t *acc) {
+    *acc += count * sizeof(T);
+    return cudaMalloc(reinterpret_cast<void **>(ptr), std::max<size_t>(count, 1) * sizeof(T));
+}
+
+template <class T>
+void dfree(T *&ptr) {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+namespace pfa {
+
+cudaError_t fixed_alloc(FixedDev &d, int m, int n, int G) {
+    size_t acc = 0;
+    cudaError_t e = cudaSuccess;
+    d.m = m; d.n = n; d.G = G; d.L = ilog2(G); d.mpad = (m + 31) / 32 * 32;
+#define TRY(x) do { e = (x); if (e != cudaSuccess) return e; } while (0)
+    TRY(dalloc(&d.f0, m, &acc)); TRY(dalloc(&d.df, m, &acc)); TRY(dalloc(&d.fac, m, &acc));
+    TRY(dalloc(&d.tan_s, m, &acc)); TRY(dalloc(&d.order, m, &acc));
+    TRY(dalloc(&d.krp, G, &acc)); TRY(dalloc(&d.kcp, G, &acc));
+    TRY(dalloc(&d.hamr, G, &acc)); TRY(dalloc(&d.hamc, G, &acc));
+    TRY(dalloc(&d.tw, G, &acc)); TRY(dalloc(&d.sinc, 256 * 32, &acc));
+    TRY(dalloc(&d.p1, (size_t)n * d.mpad, &acc));
+    TRY(dalloc(&d.y1, (size_t)n * G, &acc));
+    TRY(dalloc(&d.y2, (size_t)G * G, &acc));
+    TRY(dalloc(&d.e1, G, &acc)); TRY(dalloc(&d.e2, G, &acc));
+    TRY(dalloc(&d.ctrl, 16, &acc));
+#undef TRY
+    return cudaSuccess;
+}
+
+void fixed_free(FixedDev &d) {
+    dfree(d.f0); dfree(d.df); dfree(d.fac); dfree(d.tan_s); dfree(d.order); dfree(d.krp); dfree(d.kcp);
+    dfree(d.hamr); dfree(d.hamc); dfree(d.tw); dfree(d.sinc); dfree(d.p1); dfree(d.y1); dfree(d.y2);
+    dfree(d.e1); dfree(d.e2); dfree(d.ctrl);
+}
+
+}  // namespace pfa
+
+extern "C" {
+
+const char *pfa_version(void) { return "pfa_b200 0.1 (sm_100a)"; }
+
+const char *pfa_status_string(pfa_status st) {
+    switch (st) {
+        case PFA_OK: return "ok";
+        case PFA_ERR_BAD_CONFIG: return "bad config";
+        case PFA_ERR_BAD_DIMS: return "grid smaller than scene dims";
+        case PFA_ERR_BAD_ARG: return "bad argument";
+        case PFA_ERR_NOT_READY: return "job not set";
+        case PFA_ERR_CUDA: return "cuda error";
+        case PFA_ERR_ALLOC: return "device allocation failed";
+        case PFA_ERR_TIMEOUT: return "timeout";
+        case PFA_ERR_NO_DEVICE: return "no usable device";
+    }
+    return "unknown status";
+}
+
+pfa_status pfa_last_error(const pfa_plan *plan, char *buf, size_t len) {
+    if (!plan || !buf || len == 0) return PFA_ERR_BAD_ARG;
+    std::snprintf(buf, len, "%s", plan->err.c_str());
+    return PFA_OK;
+}
+
+pfa_status pfa_plan_create(const pfa_config *cfg, pfa_plan **out) {
+    if (!cfg || !out) return PFA_ERR_BAD_ARG;
+    *out = nullptr;
+    const pfa_config c = *cfg;
+    if (c.m < 2 || c.n < 2) return PFA_ERR_BAD_DIMS;
+    if ((c.range_interp != PFA_INTERP_LERP && c.range_interp != PFA_INTERP_SINC) ||
+        (c.az_interp != PFA_INTERP_LERP && c.az_interp != PFA_INTERP_SINC))
+        return PFA_ERR_BAD_CONFIG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= c.device || c.device < 0) return PFA_ERR_NO_DEVICE;
+    pfa_plan *p = new (std::nothrow) pfa_plan();
+    if (!p) return PFA_ERR_ALLOC;
+    p->cfg = c;
+    p->device = c.device;
+    DeviceGuard dg(c.device);
+    cudaError_t e;
+    if (c.mode == PFA_MODE_FIXED) {
+        if (!is_pow2(c.grid) || c.grid < 64 || c.grid > 16384) { delete p; return PFA_ERR_BAD_CONFIG; }
+        if (c.grid < c.m || c.grid < c.n) { delete p; return PFA_ERR_BAD_DIMS; }
+        e = pfa::fixed_alloc(p->fx, c.m, c.n, c.grid);
+        p->fx.range_sinc = c.range_interp == PFA_INTERP_SINC;
+        p->fx.az_sinc = c.az_interp == PFA_INTERP_SINC;
+        p->ws_bytes = pfa::fixed_workspace_bytes(c.m, c.n, c.grid);
+    } else if (c.mode == PFA_MODE_FLOAT32 || c.mode == PFA_MODE_MIXED) {
+        e = pfa::float_alloc(p->fl, c.m, c.n);
+        p->fl.range_sinc = c.range_interp == PFA_INTERP_SINC;
+        p->fl.az_sinc = c.az_interp == PFA_INTERP_SINC;
+        p->ws_bytes = pfa::float_workspace_bytes(c.m, c.n);
+        if (e == cudaErrorInvalidValue) { pfa::float_free(p->fl); delete p; return PFA_ERR_BAD_CONFIG; }
+    } else {
+        delete p;
+        return PFA_ERR_BAD_CONFIG;
+    }
+    if (e != cudaSuccess) {
+        pfa::fixed_free(p->fx);
+        pfa::float_free(p->fl);
+        pfa_status st = e == cudaErrorMemoryAllocation ? PFA_ERR_ALLOC : PFA_ERR_CUDA;
+        delete p;
+        return st;
+    }
+    *out = p;
+    return PFA_OK;
+}
+
+pfa_status pfa_plan_destroy(pfa_plan *p) {
+    if (!p) return PFA_ERR_BAD_ARG;
+    {
+        DeviceGuard dg(p->device);
+        pfa::fixed_free(p->fx);
+        pfa::float_free(p->fl);
+        if (p->staging_in) cudaFree(p->staging_in);
+        if (p->staging_out) cudaFree(p->staging_out);
+        if (p->host_stream) cudaStreamDestroy(p->host_stream);
+    }
+    delete p;
+    return PFA_OK;
+}
+
+size_t pfa_plan_workspace_bytes(const pfa_plan *p) { return p ? p->ws_bytes : 0; }
+
+pfa_status pfa_set_fixed_job(pfa_plan *p, const pfa_fixed_job *job) {
+    if (!p || !job) return PFA_ERR_BAD_ARG;
+    if (p->cfg.mode != PFA_MODE_FIXED) return fail(p, PFA_ERR_BAD_CONFIG, "plan is not fixed mode");
+    if (!job->f0 || !job->df || !job->pr || !job->tan_s || !job->inv_order || !job->kr_grid || !job->kc_grid)
+        return fail(p, PFA_ERR_BAD_ARG, "missing job vector");
+    DeviceGuard dg(p->device);
+    pfa::FixedDev &d = p->fx;
+    const int m = d.m, G = d.G;
+    // pass-1 source scale f32(f32(2 pr) / f32(c)) (NumPy 2 float32 arithmetic, silicon_emulator.py:144)
+    std::vector<float> fac(m);
+    const float c32 = (float)299792458.0;
+    for (int i = 0; i < m; ++i) {
+        volatile float two_pr = 2.0f * job->pr[i];
+        fac[i] = two_pr / c32;
+    }
+    // sorted slot -> pulse (inverse of inv_order); reject non-permutations
+    std::vector<int32_t> order(m, -1);
+    for (int i = 0; i < m; ++i) {
+        const int r = job->inv_order[i];
+        if (r < 0 || r >= m || order[r] != -1) return fail(p, PFA_ERR_BAD_ARG, "inv_order is not a permutation");
+        order[r] = i;
+    }
+    std::vector<int32_t> hr(G), hc(G);
+    if (job->ham_r) std::memcpy(hr.data(), job->ham_r, sizeof(int32_t) * G); else pfa::build_hamming_q15(d.n, G, hr.data());
+    if (job->ham_c) std::memcpy(hc.data(), job->ham_c, sizeof(int32_t) * G); else pfa::build_hamming_q15(m, G, hc.data());
+    std::vector<int16_t> tw2(G);
+    if (job->twiddle) std::memcpy(tw2.data(), job->twiddle, sizeof(int16_t) * G); else pfa::build_twiddles_q15(G, tw2.data());
+    // stage-contiguous layout: stage s (span 2^s) entries k < 2^(s-1) at offset 2^(s-1)-1
+    std::vector<uint32_t> tws(G, 0u);
+    const int L = d.L;
+    for (int b = 0; b < L; ++b) {
+        for (int k = 0; k < (1 << b); ++k) {
+            const int src = k << (L - 1 - b);
+            tws[(1 << b) - 1 + k] = (uint32_t)(uint16_t)tw2[2 * src] | ((uint32_t)(uint16_t)tw2[2 * src + 1] << 16);
+        }
+    }
+    std::vector<int16_t> sinc(256 * 32);
+    if (job->sinc_q15) std::memcpy(sinc.data(), job->sinc_q15, sizeof(int16_t) * 256 * 32); else pfa::build_sinc_table(sinc.data());
+    cudaError_t e;
+#define CPY(dst, src, cnt) do { e = cudaMemcpy(dst, src, sizeof(*(dst)) * (cnt), cudaMemcpyHostToDevice); \
+        if (e != cudaSuccess) return cuda_fail(p, e, "job upload"); } while (0)
+    CPY(d.f0, job->f0, m); CPY(d.df, job->df, m); CPY(d.fac, fac.data(), m); CPY(d.tan_s, job->tan_s, m);
+    CPY(d.order, order.data(), m); CPY(d.krp, job->kr_grid, G); CPY(d.kcp, job->kc_grid, G);
+    CPY(d.hamr, hr.data(), G); CPY(d.hamc, hc.data(), G); CPY(d.tw, tws.data(), G);
+    CPY(d.sinc, sinc.data(), 256 * 32);
+#undef CPY
+    p->job_ready = true;
+    return PFA_OK;
+}
+
+static pfa_status fixed_common(pfa_plan *p, const float *sig, const int16_t *iq, uint16_t *img, void *stream) {
+    if (!p || !img || (!sig && !iq)) return PFA_ERR_BAD_ARG;
+    if (p->cfg.mode != PFA_MODE_FIXED) return fail(p, PFA_ERR_BAD_CONFIG, "plan is not fixed mode");
+    if (!p->job_ready) return fail(p, PFA_ERR_NOT_READY, "pfa_set_fixed_job not called");
+    if (sig && (reinterpret_cast<uintptr_t>(sig) & 15)) return fail(p, PFA_ERR_BAD_ARG, "signal must be 16-byte aligned");
+    if (iq && (reinterpret_cast<uintptr_t>(iq) & 3)) return fail(p, PFA_ERR_BAD_ARG, "iq16 signal must be 4-byte aligned");
+    DeviceGuard dg(p->device);
+    cudaError_t e = pfa::fixed_form(p->fx, sig, reinterpret_cast<const uint32_t *>(iq), img,
+                                    reinterpret_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(p, e, "fixed form");
+    return PFA_OK;
+}
+
+pfa_status pfa_form_fixed(pfa_plan *p, const float *sig_dev, uint16_t *img_dev, void *stream) {
+    return fixed_common(p, sig_dev, nullptr, img_dev, stream);
+}
+
+pfa_status pfa_form_fixed_iq16(pfa_plan *p, const int16_t *sig_iq_dev, uint16_t *img_dev, void *stream) {
+    return fixed_common(p, nullptr, sig_iq_dev, img_dev, stream);
+}
+
+static pfa_status ensure_staging(pfa_plan *p, size_t in_bytes, size_t out_bytes) {
+    cudaError_t e;
+    if (!p->host_stream) {
+        e = cudaStreamCreateWithFlags(&p->host_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(p, e, "stream create");
+    }
+    if (p->staging_in_bytes < in_bytes) {
+        if (p->staging_in) cudaFree(p->staging_in);
+        p->staging_in = nullptr;
+        e = cudaMalloc(reinterpret_cast<void **>(&p->staging_in), in_bytes);
+        if (e != cudaSuccess) { p->staging_in_bytes = 0; return cuda_fail(p, e, "staging alloc"); }
+        p->staging_in_bytes = in_bytes;
+    }
+    if (p->staging_out_bytes < out_bytes) {
+        if (p->staging_out) cudaFree(p->staging_out);
+        p->staging_out = nullptr;
+        e = cudaMalloc(&p->staging_out, out_bytes);
+        if (e != cudaSuccess) { p->staging_out_bytes = 0; return cuda_fail(p, e, "staging alloc"); }
+        p->staging_out_bytes = out_bytes;
+    }
+    return PFA_OK;
+}
+
+pfa_status pfa_form_fixed_host(pfa_plan *p, const float *sig_host, uint16_t *img_host) {
+    if (!p || !sig_host || !img_host) return PFA_ERR_BAD_ARG;
+    if (p->cfg.mode != PFA_MODE_FIXED) return fail(p, PFA_ERR_BAD_CONFIG, "plan is not fixed mode");
+    DeviceGuard dg(p->device);
+    const size_t in_b = sizeof(float) * 2 * (size_t)p->fx.m * p->fx.n;
+    const size_t out_b = sizeof(uint16_t) * (size_t)p->fx.G * p->fx.G;
+    pfa_status st = ensure_staging(p, in_b, out_b);
+    if (st != PFA_OK) return st;
+    cudaError_t e = cudaMemcpyAsync(p->staging_in, sig_host, in_b, cudaMemcpyHostToDevice, p->host_stream);
+    if (e != cudaSuccess) return cuda_fail(p, e, "h2d");
+    st = fixed_common(p, p->staging_in, nullptr, static_cast<uint16_t *>(p->staging_out), p->host_stream);
+    if (st != PFA_OK) return st;
+    e = cudaMemcpyAsync(img_host, p->staging_out, out_b, cudaMemcpyDeviceToHost, p->host_stream);
+    if (e != cudaSuccess) return cuda_fail(p, e, "d2h");
+    e = cudaStreamSynchronize(p->host_stream);
+    if (e != cudaSuccess) return cuda_fail(p, e, "sync");
+    return PFA_OK;
+}
+
+pfa_status pfa_get_fixed_exponents(pfa_plan *p, int32_t *e_range, int32_t *e_az, int32_t *q0_exp) {
+    if (!p) return PFA_ERR_BAD_ARG;
+    if (p->cfg.mode != PFA_MODE_FIXED) return fail(p, PFA_ERR_BAD_CONFIG, "plan is not fixed mode");
+    DeviceGuard dg(p->device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(p, e, "sync");
+    if (e_range && (e = cudaMemcpy(e_range, p->fx.e1, sizeof(int32_t) * p->fx.n, cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return cuda_fail(p, e, "exponents");
+    if (e_az && (e = cudaMemcpy(e_az, p->fx.e2, sizeof(int32_t) * p->fx.G, cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return cuda_fail(p, e, "exponents");
+    if (q0_exp) {
+        int32_t ctrl[4];
+        if ((e = cudaMemcpy(ctrl, p->fx.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost)) != cudaSuccess)
+            return cuda_fail(p, e, "exponents");
+        *q0_exp = ctrl[3];
+    }
+    return PFA_OK;
+}
+
+}  // extern "C"

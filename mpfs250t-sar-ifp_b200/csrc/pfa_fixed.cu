@@ -1,0 +1,655 @@
+// Fixed-point PFA datapath on sm_100a, bit-exact to the reference emulator
+// (mpfs/host/silicon_emulator.py:226-249).
+//
+// Kernels (one stream, stream-ordered):
+//   k_q0max        block max of |re|,|im| over the complex64 signal (fixedpoint.fit_scale, :19-26)
+//   k_fx_pass1     Q0 quantise + pass-1 bracket search (FP64) + 32-tap sinc / 2-tap lerp gather per
+//                  pulse; a 32-slot x 256-bin shared tile turns the pulse-major output into range-bin
+//                  rows (corner turn #1, silicon_emulator.py:142-148)
+//   k_fx_pass2_fft pass-2 bracket search + gather + Q15 window + 13-stage per-row BFP FFT along the
+//                  cross axis (silicon_emulator.py:150-156, 165-195, 198-205 with fixedpoint.py:266-289)
+//   k_fx_fft2      renormalise FFT-1 rows by (emax - e_row) on load, BFP FFT along range
+//                  (corner turn #2 by strided column reads, silicon_emulator.py:241-245)
+//   k_fx_detect    renormalise FFT-2 rows, integer |z|, transpose to [range][cross] (:247-249, :208-213)
+//
+// Exactness notes.  Every floating step the emulator takes is reproduced with the same IEEE
+// operation: __dmul_rn/__dadd_rn/__ddiv_rn (no FMA contraction) for the float64 coordinates and
+// fractions, __fmul_rn/__fdiv_rn where NumPy 2 computes in float32 (pass-1 source scale, pass-2
+// source coordinates, the Q0 division, the pass-1 lerp product), rint() for np.round.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "pfa_internal.h"
+
+namespace pfa {
+namespace {
+
+constexpr int kSincTaps = 32;
+constexpr int kSincFirst = -15;
+
+__device__ __forceinline__ int sat16(int v) { return min(max(v, -32768), 32767); }
+__device__ __forceinline__ long long sat16ll(long long v) { return v < -32768 ? -32768 : (v > 32767 ? 32767 : v); }
+__device__ __forceinline__ uint32_t pack16(int re, int im) {
+    return (uint32_t)(uint16_t)re | ((uint32_t)(uint16_t)im << 16);
+}
+__device__ __forceinline__ int lo16(uint32_t p) { return (int)(int16_t)(p & 0xffffu); }
+__device__ __forceinline__ int hi16(uint32_t p) { return (int)(int16_t)(p >> 16); }
+__device__ __forceinline__ int wrap16(int v) { return (int)(int16_t)(v & 0xffff); }
+
+// Smallest e with M <= 32767 * 2^e, i.e. ceil(log2(M / 32767)) of fixedpoint.fit_scale for a float32
+// maximum M (exact: M/32767 is either an exact power of two or at least 2^-24 away from one).
+__device__ __forceinline__ int q0_exponent(uint32_t bits) {
+    float M = __uint_as_float(bits);
+    if (!(M > 0.0f)) return 0;
+    double md = (double)M;
+    int e = ilogb(md) - 15;
+    while (md > ldexp(32767.0, e)) ++e;
+    return e;
+}
+
+// floor(x / lsb) in float32 (the emulator divides float32 planes by a weak float scalar), sat16.
+__device__ __forceinline__ int q0_quantise(float x, float lsb) {
+    return sat16((int)fmaxf(fminf(floorf(__fdiv_rn(x, lsb)), 32767.0f), -32768.0f));
+}
+
+// lower_bound over a non-decreasing sequence xa(0..n-1): first t with xa(t) >= q (n if none).
+// Starts from a guess and walks; falls back to bisection after a few steps.
+template <class F>
+__device__ __forceinline__ int lower_bound_from(const F &xa, int n, double q, int g) {
+    int t = min(max(g, 0), n);
+    int steps = 0;
+    while (t < n && xa(t) < q) {
+        ++t;
+        if (++steps > 6) {
+            int lo = t, hi = n;
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (xa(mid) < q) lo = mid + 1; else hi = mid;
+            }
+            return lo;
+        }
+    }
+    while (t > 0 && xa(t - 1) >= q) {
+        --t;
+        if (++steps > 6) {
+            int lo = 0, hi = t;
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (xa(mid) < q) lo = mid + 1; else hi = mid;
+            }
+            return lo;
+        }
+    }
+    return t;
+}
+
+struct Bracket {
+    int idx;   // natural-order lower index, -1 = out of span
+    int wq;    // Q15 weight
+};
+
+// interp_coeffs (serialize_inputs.py:67-94) for one query, given the count of ascending-view
+// source coordinates below q and an accessor of the ascending view.
+template <class F>
+__device__ __forceinline__ Bracket bracket_from_count(const F &xa, int n, bool asc, double q, int cnt) {
+    Bracket b{-1, 0};
+    int k = cnt - 1;
+    if (k < 0 || k >= n - 1) return b;
+    double x0 = xa(k), x1 = xa(k + 1);
+    double fa = __ddiv_rn(__dsub_rn(q, x0), __dsub_rn(x1, x0));
+    double w = asc ? fa : __dsub_rn(1.0, fa);
+    double r = rint(__dmul_rn(w, 32768.0));
+    r = fmin(fmax(r, 0.0), 32767.0);
+    b.idx = asc ? k : (n - 2 - k);
+    b.wq = (int)r;
+    return b;
+}
+
+// 32-tap sinc / edge lerp / zero of apply_sinc (silicon_emulator.py:88-122) on a window of packed
+// int16x2 samples; `win` is indexed by (source index - base).
+__device__ __forceinline__ uint32_t sinc_gather(const uint32_t *win, int base, int sn, Bracket b,
+                                                const int16_t *tab) {
+    if (b.idx < 0) return 0u;
+    if (b.idx >= -kSincFirst && b.idx <= sn - (kSincTaps + kSincFirst)) {
+        const int16_t *c = tab + (b.wq >> 7) * kSincTaps;
+        const uint32_t *x = win + (b.idx + kSincFirst - base);
+        long long ar = 0, ai = 0;
+#pragma unroll
+        for (int t = 0; t < kSincTaps; ++t) {
+            const int ct = c[t];
+            const uint32_t v = x[t];
+            ar += (long long)(ct * 1) * lo16(v);
+            ai += (long long)(ct * 1) * hi16(v);
+        }
+        return pack16((int)sat16ll((ar + (1 << 14)) >> 15), (int)sat16ll((ai + (1 << 14)) >> 15));
+    }
+    const uint32_t va = win[b.idx - base], vb = win[b.idx + 1 - base];
+    const int ar = lo16(va), ai = hi16(va), br = lo16(vb), bi = hi16(vb);
+    return pack16(sat16(ar + (((br - ar) * b.wq) >> 15)), sat16(ai + (((bi - ai) * b.wq) >> 15)));
+}
+
+// apply_fixed (silicon_emulator.py:60-71).  F32PROD: the product (b-a)*wq rounded to float32, as in
+// pass 1 where the emulator's quantised signal is complex64.
+template <bool F32PROD>
+__device__ __forceinline__ uint32_t lerp_gather(const uint32_t *win, int base, Bracket b) {
+    if (b.idx < 0) return 0u;
+    const uint32_t va = win[b.idx - base], vb = win[b.idx + 1 - base];
+    const int ar = lo16(va), ai = hi16(va), br = lo16(vb), bi = hi16(vb);
+    int sr, si;
+    if (F32PROD) {
+        const float w = (float)b.wq;
+        sr = (int)floorf(__fmul_rn(__fmul_rn((float)(br - ar), w), 1.0f / 32768.0f));
+        si = (int)floorf(__fmul_rn(__fmul_rn((float)(bi - ai), w), 1.0f / 32768.0f));
+    } else {
+        sr = ((br - ar) * b.wq) >> 15;
+        si = ((bi - ai) * b.wq) >> 15;
+    }
+    return pack16(sat16(ar + sr), sat16(ai + si));
+}
+
+// ------------------------------------------------------------------------------------------ K0
+__global__ void k_q0max(const float4 *__restrict__ sig4, long long n4, const float *__restrict__ tail,
+                        int ntail, uint32_t *__restrict__ out_bits) {
+    float mx = 0.0f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float4 v = __ldcs(sig4 + i);
+        mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+    }
+    if (blockIdx.x == 0 && threadIdx.x < ntail) mx = fmaxf(mx, fabsf(tail[threadIdx.x]));
+    uint32_t b = __reduce_max_sync(0xffffffffu, __float_as_uint(mx));
+    if ((threadIdx.x & 31) == 0) atomicMax(out_bits, b);
+}
+
+__global__ void k_q0exp(int32_t *ctrl) { ctrl[3] = q0_exponent((uint32_t)ctrl[0]); }
+
+// ------------------------------------------------------------------------------------------ K1
+constexpr int P1_SLOTS = 32;          // sorted pulse slots per CTA
+constexpr int P1_BINS = 256;          // range bins per CTA
+constexpr int P1_WARPS = 8;
+constexpr int P1_WMAX = 512;          // per-warp source window (samples)
+
+struct Pass1Args {
+    const float2 *sig;                // complex64 input (or nullptr)
+    const uint32_t *sig_iq;           // packed int16 I/Q input (or nullptr)
+    const float *f0, *df, *fac, *krp;
+    const int32_t *order;
+    const int16_t *sinc;
+    const int32_t *ctrl;
+    uint32_t *p1;
+    int m, n, mpad;
+};
+
+constexpr size_t P1_SMEM_TILE = (size_t)P1_BINS * (P1_SLOTS + 1) * 4;
+constexpr size_t P1_SMEM_WIN = (size_t)P1_WARPS * P1_WMAX * 4;
+constexpr size_t p1_smem(bool sinc) { return P1_SMEM_TILE + P1_SMEM_WIN + (sinc ? 2 * 256 * kSincTaps : 0); }
+
+template <bool SINC>
+__global__ void __launch_bounds__(256) k_fx_pass1(Pass1Args a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t(*tile)[P1_SLOTS + 1] = reinterpret_cast<uint32_t(*)[P1_SLOTS + 1]>(smem);
+    uint32_t(*win)[P1_WMAX] = reinterpret_cast<uint32_t(*)[P1_WMAX]>(smem + P1_SMEM_TILE);
+    int16_t *tab = reinterpret_cast<int16_t *>(smem + P1_SMEM_TILE + P1_SMEM_WIN);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int r0 = blockIdx.x * P1_SLOTS;
+    const int j0 = blockIdx.y * P1_BINS;
+    const int n = a.n;
+    if (SINC) {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(a.sinc);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(tab);
+        for (int i = tid; i < 256 * kSincTaps / 2; i += blockDim.x) dst[i] = src[i];
+    }
+    const float lsb = a.sig ? (float)ldexp(1.0, a.ctrl[3]) : 1.0f;
+    __syncthreads();
+
+    for (int s = 0; s < P1_SLOTS / P1_WARPS; ++s) {
+        const int slot = warp + P1_WARPS * s;
+        const int r = r0 + slot;
+        if (r >= a.m) {
+            for (int t = lane; t < P1_BINS; t += 32) tile[t][slot] = 0u;
+            continue;
+        }
+        const int i = a.order[r];
+        const double fac = (double)a.fac[i], f0 = (double)a.f0[i], df = (double)a.df[i];
+        // kr_i[k] = f64(fac) * (f64(f0) + f64(k) * f64(df))   (silicon_emulator.py:144)
+        auto kr = [&](int k) { return __dmul_rn(fac, __dadd_rn(f0, __dmul_rn((double)k, df))); };
+        const bool asc = kr(n - 1) >= kr(0);
+        auto xa = [&](int t) { return asc ? kr(t) : kr(n - 1 - t); };
+        const double inv_step = 1.0 / (fac * df);     // affine-estimate coefficients (guess only)
+        const double c0 = f0 / df;
+        Bracket br[P1_BINS / 32];
+        int lo_i = 1 << 30, hi_i = -1;
+#pragma unroll
+        for (int t = 0; t < P1_BINS / 32; ++t) {
+            const int j = j0 + lane + 32 * t;
+            br[t] = Bracket{-1, 0};
+            if (j < n) {
+                const double q = (double)a.krp[j];
+                const double kest = q * inv_step - c0;     // affine estimate of the source index
+                int g = 0;
+                if (isfinite(kest) && isfinite(inv_step)) {
+                    const double tt = asc ? ceil(kest) : ceil((double)(n - 1) - kest);
+                    g = (int)fmin(fmax(tt, -1.0), (double)n + 1.0);
+                }
+                const int cnt = lower_bound_from(xa, n, q, g);
+                br[t] = bracket_from_count(xa, n, asc, q, cnt);
+                if (br[t].idx >= 0) {
+                    lo_i = min(lo_i, br[t].idx);
+                    hi_i = max(hi_i, br[t].idx);
+                }
+            }
+        }
+        lo_i = __reduce_min_sync(0xffffffffu, lo_i);
+        hi_i = __reduce_max_sync(0xffffffffu, hi_i);
+        int wlo = 0, whi = 0;
+        if (hi_i >= 0) {
+            wlo = max(0, lo_i + (SINC ? kSincFirst : 0));
+            whi = min(n, hi_i + (SINC ? kSincTaps + kSincFirst : 2));
+        }
+        const bool fits = (whi - wlo) <= P1_WMAX;
+        uint32_t *w = win[warp];
+        if (fits) {
+            for (int k = wlo + lane; k < whi; k += 32) {
+                const size_t off = (size_t)i * n + k;
+                uint32_t v;
+                if (a.sig) {
+                    const float2 z = a.sig[off];
+                    v = pack16(q0_quantise(z.x, lsb), q0_quantise(z.y, lsb));
+                } else {
+                    v = a.sig_iq[off];
+                }
+                w[k - wlo] = v;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < P1_BINS / 32; ++t) {
+            const int jj = lane + 32 * t;
+            uint32_t out = 0u;
+            if (j0 + jj < n && br[t].idx >= 0) {
+                if (fits) {
+                    out = SINC ? sinc_gather(w, wlo, n, br[t], tab) : lerp_gather<true>(w, wlo, br[t]);
+                } else {
+                    // Window wider than the staging buffer: gather straight from global memory.
+                    uint32_t tmp[kSincTaps + 1];
+                    const int base = SINC ? max(0, br[t].idx + kSincFirst) : br[t].idx;
+                    const int cnt = SINC ? min(n, br[t].idx + kSincTaps + kSincFirst) - base : 2;
+                    for (int u = 0; u < cnt; ++u) {
+                        const size_t off = (size_t)i * n + base + u;
+                        if (a.sig) {
+                            const float2 z = a.sig[off];
+                            tmp[u] = pack16(q0_quantise(z.x, lsb), q0_quantise(z.y, lsb));
+                        } else {
+                            tmp[u] = a.sig_iq[off];
+                        }
+                    }
+                    out = SINC ? sinc_gather(tmp, base, n, br[t], tab) : lerp_gather<true>(tmp, base, br[t]);
+                }
+            }
+            tile[jj][slot] = out;
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // corner turn #1: range-bin rows, sorted-slot columns, 128 B per row segment
+    for (int jj = warp; jj < P1_BINS; jj += P1_WARPS) {
+        const int j = j0 + jj;
+        if (j >= n) break;
+        const int r = r0 + lane;
+        if (r < a.mpad) a.p1[(size_t)j * a.mpad + r] = tile[jj][lane];
+    }
+}
+
+// ------------------------------------------------------------------------------------------ BFP FFT
+// Per-row block-floating-point radix-2 DIT FFT of fixedpoint.fft1d_bfp_hw_perrow (fixedpoint.py:266-289)
+// held in registers: E values per thread, T = N/E threads.  Stages whose butterfly bit lies in a
+// thread's register bits run in registers; between bit groups the row is exchanged through shared
+// memory.  After every stage the row max of |re|,|im| sets the conditional shift (the same for every
+// layout, so the per-stage arithmetic is identical to the reference).
+//
+// Positions p are those of the bit-reversed working array.  Group g with bit range [lo, lo+LE):
+// element v of logical thread t sits at p = (t & (2^lo - 1)) | v << lo | (t >> lo) << (lo + LE).
+// Group 0 uses logical t = bitrev(tid), so its element v holds natural input index tid + T*bitrev(v).
+template <int L, int E>
+struct BfpFft {
+    static constexpr int N = 1 << L;
+    static constexpr int LE = (E == 16) ? 4 : (E == 8) ? 3 : (E == 4) ? 2 : 1;
+    static constexpr int T = N / E;
+    static constexpr int TB = L - LE;        // thread bits
+    static constexpr int WARPS = T / 32;
+    static constexpr int NG = (L + LE - 1) / LE;
+    static_assert(T >= 32, "at least one warp");
+
+    __device__ static __forceinline__ int group_lo(int g) {
+        return (g * LE + LE <= L) ? g * LE : (L - LE);
+    }
+    __device__ static __forceinline__ int pos(int lo, int t, int v) {
+        return (t & ((1 << lo) - 1)) | (v << lo) | ((t >> lo) << (lo + LE));
+    }
+    __device__ static __forceinline__ int swz(int p) { return p + (p >> 5); }
+    __device__ static __forceinline__ int logical(int g, int tid) {
+        return g == 0 ? (int)(__brev((unsigned)tid) >> (32 - TB)) : tid;
+    }
+
+    // Runs the full transform on xr/xi (group-0 layout in, last-group layout out).  Returns e_row.
+    __device__ static int run(int (&xr)[E], int (&xi)[E], uint32_t *xbuf, const uint32_t *tw,
+                              int (*red)[32], int tid) {
+        int e_row = 0;
+        int done = 0;
+        int rbuf = 0;
+        const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+        for (int g = 0; g < NG; ++g) {
+            const int lo = group_lo(g);
+            const int t = logical(g, tid);
+            if (g > 0) {
+                // exchange: write in group g-1 layout, read in group g layout
+                const int plo = group_lo(g - 1);
+                const int pt = logical(g - 1, tid);
+#pragma unroll
+                for (int v = 0; v < E; ++v) xbuf[swz(pos(plo, pt, v))] = pack16(xr[v], xi[v]);
+                __syncthreads();
+#pragma unroll
+                for (int v = 0; v < E; ++v) {
+                    const uint32_t u = xbuf[swz(pos(lo, t, v))];
+                    xr[v] = lo16(u);
+                    xi[v] = hi16(u);
+                }
+            }
+            const int tlow = t & ((1 << lo) - 1);
+#pragma unroll
+            for (int rb = 0; rb < LE; ++rb) {
+                const int b = lo + rb;
+                if (b < done) continue;
+                // stage s = b + 1: pairs (p, p + 2^b); twiddle k = p mod 2^b from the stage table
+                const uint32_t *tws = tw + ((1 << b) - 1);
+                unsigned mx = 0;
+#pragma unroll
+                for (int v = 0; v < E; ++v) {
+                    if (v & (1 << rb)) continue;
+                    const int v2 = v | (1 << rb);
+                    const int k = tlow | ((v & ((1 << rb) - 1)) << lo);
+                    const uint32_t w = tws[k];
+                    const int wr = lo16(w), wi = hi16(w);
+                    const int br = xr[v2], bi = xi[v2];
+                    const int tr = sat16((wr * br - wi * bi) >> 15);
+                    const int ti = sat16((wr * bi + wi * br) >> 15);
+                    const int ar = xr[v], ai = xi[v];
+                    xr[v] = ar + tr;
+                    xi[v] = ai + ti;
+                    xr[v2] = ar - tr;
+                    xi[v2] = ai - ti;
+                }
+#pragma unroll
+                for (int v = 0; v < E; ++v) {
+                    mx = max(mx, (unsigned)max(abs(xr[v]), abs(xi[v])));
+                }
+                mx = __reduce_max_sync(0xffffffffu, mx);
+                if (lane == 0) red[rbuf][warp] = (int)mx;
+                __syncthreads();
+                int rowmax = 0;
+#pragma unroll
+                for (int q = 0; q < WARPS; ++q) rowmax = max(rowmax, red[rbuf][q]);
+                rbuf ^= 1;
+                // max(0, ceil(log2((mx + 1) / 32767))) on integers
+                int sh = 0;
+                while ((long long)rowmax + 1 > (32767LL << sh)) ++sh;
+                if (sh) {
+#pragma unroll
+                    for (int v = 0; v < E; ++v) {
+                        xr[v] = sat16(xr[v] >> sh);
+                        xi[v] = sat16(xi[v] >> sh);
+                    }
+                }
+                e_row += sh;
+            }
+            done = lo + LE;
+        }
+        return e_row;
+    }
+    // Output position of element v after run(): p = tid | v << (L - LE)
+};
+
+// ------------------------------------------------------------------------------------------ K2
+struct Pass2Args {
+    const uint32_t *p1;
+    const float *tan_s, *krp, *kcp;
+    const int32_t *hamr, *hamc;
+    const uint32_t *tw;
+    const int16_t *sinc;
+    uint32_t *y1;
+    int32_t *e1, *ctrl;
+    int m, n, mpad;
+};
+
+template <int L, int E, bool SINC>
+__global__ void __launch_bounds__((1 << L) / E) k_fx_pass2_fft(Pass2Args a) {
+    using F = BfpFft<L, E>;
+    constexpr int N = F::N, T = F::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    // layout: [region A: src coords f32[m] + row u32[m] | exchange buffer] [tw N-1] [sinc] [red]
+    const int m = a.m;
+    const size_t regA = max((size_t)8 * m, (size_t)4 * (N + N / 32));
+    float *srcx = reinterpret_cast<float *>(smem);
+    uint32_t *row = reinterpret_cast<uint32_t *>(smem + 4 * (size_t)m);
+    uint32_t *xbuf = reinterpret_cast<uint32_t *>(smem);
+    uint32_t *tw = reinterpret_cast<uint32_t *>(smem + regA);
+    int16_t *tab = reinterpret_cast<int16_t *>(smem + regA + 4 * (size_t)N);
+    int(*red)[32] = reinterpret_cast<int(*)[32]>(smem + regA + 4 * (size_t)N + (SINC ? 2 * 256 * kSincTaps : 0));
+
+    const int tid = threadIdx.x;
+    const int j = blockIdx.x;                       // range bin (< n)
+    const float krj = a.krp[j];
+    for (int r = tid; r < m; r += T) {
+        srcx[r] = __fmul_rn(krj, a.tan_s[r]);      // KRp[j] * tan_s in float32 (silicon_emulator.py:152)
+        row[r] = a.p1[(size_t)j * a.mpad + r];
+    }
+    for (int i = tid; i < N - 1; i += T) tw[i] = a.tw[i];
+    if (SINC) {
+        const uint32_t *s = reinterpret_cast<const uint32_t *>(a.sinc);
+        uint32_t *d = reinterpret_cast<uint32_t *>(tab);
+        for (int i = tid; i < 256 * kSincTaps / 2; i += T) d[i] = s[i];
+    }
+    __syncthreads();
+
+    const bool asc = srcx[m - 1] >= srcx[0];
+    auto xa = [&](int t) { return (double)(asc ? srcx[t] : srcx[m - 1 - t]); };
+    const double lo_v = xa(0), hi_v = xa(m - 1);
+    const double inv_span = (double)(m - 1) / (hi_v - lo_v);
+    const int hr = a.hamr[j];
+
+    int xr[E], xi[E];
+#pragma unroll
+    for (int u = 0; u < E; ++u) {
+        const int k = tid + T * u;                  // natural cross index
+        const double q = (double)a.kcp[k];
+        Bracket b{-1, 0};
+        if (q > lo_v && q <= hi_v) {
+            const int g = (int)((q - lo_v) * inv_span) + 1;
+            const int cnt = lower_bound_from(xa, m, q, g);
+            b = bracket_from_count(xa, m, asc, q, cnt);
+        }
+        const uint32_t v = SINC ? sinc_gather(row, 0, m, b, tab) : lerp_gather<false>(row, 0, b);
+        // window_fixed: cw = (int16)((hr * hc) >> 15); out = (int16)((x * cw) >> 15)
+        const int cw = wrap16((hr * a.hamc[k]) >> 15);
+        const int wr = wrap16((lo16(v) * cw) >> 15);
+        const int wi = wrap16((hi16(v) * cw) >> 15);
+        const int vv = (int)(__brev((unsigned)u) >> (32 - F::LE));
+        xr[vv] = wr;
+        xi[vv] = wi;
+    }
+    __syncthreads();                                // region A becomes the exchange buffer
+    const int e_row = F::run(xr, xi, xbuf, tw, red, tid);
+    uint32_t *out = a.y1 + (size_t)j * N;
+#pragma unroll
+    for (int v = 0; v < E; ++v) out[tid + T * v] = pack16(xr[v], xi[v]);
+    if (tid == 0) {
+        a.e1[j] = e_row;
+        atomicMax(a.ctrl + 1, e_row);
+    }
+}
+
+// ------------------------------------------------------------------------------------------ K3
+struct Fft2Args {
+    const uint32_t *y1;
+    const int32_t *e1;
+    const uint32_t *tw;
+    uint32_t *y2;
+    int32_t *e2, *ctrl;
+    int n;
+};
+
+template <int L, int E>
+__global__ void __launch_bounds__((1 << L) / E) k_fx_fft2(Fft2Args a) {
+    using F = BfpFft<L, E>;
+    constexpr int N = F::N, T = F::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t *xbuf = reinterpret_cast<uint32_t *>(smem);
+    uint32_t *tw = reinterpret_cast<uint32_t *>(smem + 4 * (size_t)(N + N / 32));
+    int(*red)[32] = reinterpret_cast<int(*)[32]>(smem + 4 * (size_t)(N + N / 32) + 4 * (size_t)N);
+    const int tid = threadIdx.x;
+    const int k = blockIdx.x;                       // cross bin
+    for (int i = tid; i < N - 1; i += T) tw[i] = a.tw[i];
+    const int emax1 = a.ctrl[1];
+    int xr[E], xi[E];
+#pragma unroll
+    for (int u = 0; u < E; ++u) {
+        const int jr = tid + T * u;                 // natural range index
+        int r = 0, i = 0;
+        if (jr < a.n) {
+            const uint32_t v = __ldg(a.y1 + (size_t)jr * N + k);
+            const int s = min(emax1 - __ldg(a.e1 + jr), 31);
+            r = sat16(lo16(v) >> s);
+            i = sat16(hi16(v) >> s);
+        }
+        const int vv = (int)(__brev((unsigned)u) >> (32 - F::LE));
+        xr[vv] = r;
+        xi[vv] = i;
+    }
+    __syncthreads();
+    const int e_row = F::run(xr, xi, xbuf, tw, red, tid);
+    uint32_t *out = a.y2 + (size_t)k * N;
+#pragma unroll
+    for (int v = 0; v < E; ++v) out[tid + T * v] = pack16(xr[v], xi[v]);
+    if (tid == 0) {
+        a.e2[k] = e_row;
+        atomicMax(a.ctrl + 2, e_row);
+    }
+}
+
+// ------------------------------------------------------------------------------------------ K4
+// img[j][k] = floor(sqrt(re^2 + im^2)) of sat16(y2[k][j] >> (emax2 - e2[k])); 64x64 tiles.
+__global__ void __launch_bounds__(256) k_fx_detect(const uint32_t *__restrict__ y2, const int32_t *__restrict__ e2,
+                                                   const int32_t *__restrict__ ctrl, uint16_t *__restrict__ img, int G) {
+    __shared__ uint16_t t[64][65];
+    const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+    const int emax2 = ctrl[2];
+    const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;   // 64 x 4
+    for (int kk = ty; kk < 64; kk += 4) {
+        const int k = k0 + kk;
+        const uint32_t v = __ldcs(y2 + (size_t)k * G + j0 + tx);
+        const int s = min(emax2 - e2[k], 31);
+        const int r = sat16(lo16(v) >> s), i = sat16(hi16(v) >> s);
+        const unsigned p = (unsigned)(r * r) + (unsigned)(i * i);
+        unsigned q = (unsigned)sqrtf((float)p);
+        while (q * q > p) --q;
+        while ((q + 1) * (q + 1) <= p) ++q;
+        t[tx][kk] = (uint16_t)min(q, 65535u);
+    }
+    __syncthreads();
+    for (int jj = ty; jj < 64; jj += 4) img[(size_t)(j0 + jj) * G + k0 + tx] = t[jj][tx];
+}
+
+// ------------------------------------------------------------------------------------------ launch
+template <int L>
+struct FixedLaunch {
+    static constexpr int N = 1 << L;
+    static constexpr int E = (N >= 512) ? 16 : (N / 32);
+    static constexpr int T = N / E;
+
+    static size_t pass2_smem(int m, bool sinc) {
+        size_t regA = (size_t)8 * m;
+        size_t xb = (size_t)4 * (N + N / 32);
+        if (xb > regA) regA = xb;
+        return regA + 4 * (size_t)N + (sinc ? 2 * 256 * kSincTaps : 0) + 2 * 32 * 4;
+    }
+    static size_t fft2_smem() { return 4 * (size_t)(N + N / 32) + 4 * (size_t)N + 2 * 32 * 4; }
+
+    static cudaError_t run(const FixedDev &d, const float *sig, const uint32_t *sig_iq, uint16_t *img,
+                           cudaStream_t st) {
+        cudaError_t e;
+        // K0: Q0 block exponent
+        if (sig) {
+            const long long nf = 2LL * d.m * d.n;
+            const long long n4 = nf / 4;
+            const int ntail = (int)(nf - 4 * n4);
+            k_q0max<<<148 * 8, 256, 0, st>>>(reinterpret_cast<const float4 *>(sig), n4, sig + 4 * n4, ntail,
+                                             reinterpret_cast<uint32_t *>(d.ctrl));
+            k_q0exp<<<1, 1, 0, st>>>(d.ctrl);
+        }
+        // K1: pass 1
+        Pass1Args p1{reinterpret_cast<const float2 *>(sig), sig_iq, d.f0, d.df, d.fac, d.krp, d.order, d.sinc,
+                     d.ctrl, d.p1, d.m, d.n, d.mpad};
+        dim3 g1((d.m + P1_SLOTS - 1) / P1_SLOTS, (d.n + P1_BINS - 1) / P1_BINS);
+        if (d.range_sinc) {
+            e = cudaFuncSetAttribute(k_fx_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p1_smem(true));
+            if (e != cudaSuccess) return e;
+            k_fx_pass1<true><<<g1, 256, p1_smem(true), st>>>(p1);
+        } else {
+            e = cudaFuncSetAttribute(k_fx_pass1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p1_smem(false));
+            if (e != cudaSuccess) return e;
+            k_fx_pass1<false><<<g1, 256, p1_smem(false), st>>>(p1);
+        }
+        // K2: pass 2 + window + FFT-1
+        Pass2Args p2{d.p1, d.tan_s, d.krp, d.kcp, d.hamr, d.hamc, d.tw, d.sinc, d.y1, d.e1, d.ctrl, d.m, d.n, d.mpad};
+        const size_t s2 = pass2_smem(d.m, d.az_sinc != 0);
+        if (d.az_sinc) {
+            e = cudaFuncSetAttribute(k_fx_pass2_fft<L, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);
+            if (e != cudaSuccess) return e;
+            k_fx_pass2_fft<L, E, true><<<d.n, T, s2, st>>>(p2);
+        } else {
+            e = cudaFuncSetAttribute(k_fx_pass2_fft<L, E, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);
+            if (e != cudaSuccess) return e;
+            k_fx_pass2_fft<L, E, false><<<d.n, T, s2, st>>>(p2);
+        }
+        // K3: FFT-2 along range
+        Fft2Args f2{d.y1, d.e1, d.tw, d.y2, d.e2, d.ctrl, d.n};
+        const size_t s3 = fft2_smem();
+        e = cudaFuncSetAttribute(k_fx_fft2<L, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3);
+        if (e != cudaSuccess) return e;
+        k_fx_fft2<L, E><<<N, T, s3, st>>>(f2);
+        // K4: renorm + detect + transpose
+        dim3 g4(N / 64, N / 64);
+        k_fx_detect<<<g4, 256, 0, st>>>(d.y2, d.e2, d.ctrl, img, N);
+        return cudaGetLastError();
+    }
+};
+
+}  // namespace
+
+cudaError_t fixed_form(const FixedDev &d, const float *sig_c64, const uint32_t *sig_iq, uint16_t *img,
+                       cudaStream_t st) {
+    // reset the reduction words: q0 max, emax1, emax2
+    cudaError_t e = cudaMemsetAsync(d.ctrl, 0, 4 * sizeof(int32_t), st);
+    if (e != cudaSuccess) return e;
+    switch (d.L) {
+        case 6: return FixedLaunch<6>::run(d, sig_c64, sig_iq, img, st);
+        case 7: return FixedLaunch<7>::run(d, sig_c64, sig_iq, img, st);
+        case 8: return FixedLaunch<8>::run(d, sig_c64, sig_iq, img, st);
+        case 9: return FixedLaunch<9>::run(d, sig_c64, sig_iq, img, st);
+        case 10: return FixedLaunch<10>::run(d, sig_c64, sig_iq, img, st);
+        case 11: return FixedLaunch<11>::run(d, sig_c64, sig_iq, img, st);
+        case 12: return FixedLaunch<12>::run(d, sig_c64, sig_iq, img, st);
+        case 13: return FixedLaunch<13>::run(d, sig_c64, sig_iq, img, st);
+        case 14: return FixedLaunch<14>::run(d, sig_c64, sig_iq, img, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+size_t fixed_workspace_bytes(int m, int n, int G) {
+    const int mpad = (m + 31) / 32 * 32;
+    return (size_t)4 * n * mpad + (size_t)4 * n * G + (size_t)4 * G * G + 8 * (size_t)G + 64;
+}
+
+}  // namespace pfa

@@ -1,0 +1,83 @@
+// Internal plan state shared by the C-ABI glue and the kernel launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/pfa_b200.h"
+
+namespace pfa {
+
+// Device-resident fixed-point job + workspace for one (m, n, G) frame.
+struct FixedDev {
+    int m = 0, n = 0, G = 0, L = 0, mpad = 0;
+    int range_sinc = 0, az_sinc = 0;
+    // job vectors (device)
+    float *f0 = nullptr, *df = nullptr, *fac = nullptr, *tan_s = nullptr;
+    float *krp = nullptr, *kcp = nullptr;
+    int32_t *order = nullptr;          // sorted slot -> pulse index
+    int32_t *hamr = nullptr, *hamc = nullptr;
+    uint32_t *tw = nullptr;            // stage-contiguous twiddles, G-1 packed int16x2
+    int16_t *sinc = nullptr;           // 256 x 32
+    // workspace (device)
+    uint32_t *p1 = nullptr;            // [n][mpad] pass-1 output, packed int16x2
+    uint32_t *y1 = nullptr;            // [n][G] FFT-1 output (range-bin rows)
+    uint32_t *y2 = nullptr;            // [G][G] FFT-2 output (cross-bin rows)
+    int32_t *e1 = nullptr;             // [G]
+    int32_t *e2 = nullptr;             // [G]
+    int32_t *ctrl = nullptr;           // [0] q0 max bits, [1] emax1, [2] emax2, [3] q0 exponent
+};
+
+struct FloatDev {
+    int m = 0, n = 0, m2 = 0, n2 = 0, Lm = 0, Ln = 0, mpad = 0;
+    int range_sinc = 0, az_sinc = 0, sgn = -1, layout = 0;
+    double *f0 = nullptr, *df = nullptr, *pr = nullptr, *tan_s = nullptr, *kr = nullptr, *kc = nullptr;
+    float *ham_m = nullptr, *ham_n = nullptr;   // unused when window is off
+    double *ham_m64 = nullptr, *ham_n64 = nullptr;
+    int32_t *order = nullptr;
+    float2 *twm = nullptr, *twn = nullptr;      // stage-contiguous twiddles for m2 and n2
+    int16_t *sinc = nullptr;
+    int window = 1;
+    float2 *p1 = nullptr;              // [n][mpad] pass-1 output (range-bin rows, sorted pulses)
+    float2 *y1 = nullptr;              // [n][m2] cross FFT output (range-bin rows)
+};
+
+}  // namespace pfa
+
+struct pfa_plan {
+    pfa_config cfg{};
+    int device = 0;
+    bool job_ready = false;
+    size_t ws_bytes = 0;
+    pfa::FixedDev fx;
+    pfa::FloatDev fl;
+    float *staging_in = nullptr;       // device copy of the host signal (host entry points)
+    void *staging_out = nullptr;
+    size_t staging_in_bytes = 0, staging_out_bytes = 0;
+    cudaStream_t host_stream = nullptr;
+    std::string err;
+};
+
+namespace pfa {
+
+// Kernel launchers (pfa_fixed.cu / pfa_float.cu). They return a cudaError_t from the launches.
+cudaError_t fixed_form(const FixedDev &d, const float *sig_c64, const uint32_t *sig_iq, uint16_t *img,
+                       cudaStream_t st);
+size_t fixed_workspace_bytes(int m, int n, int G);
+cudaError_t fixed_alloc(FixedDev &d, int m, int n, int G);
+void fixed_free(FixedDev &d);
+
+cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int detect, cudaStream_t st);
+size_t float_workspace_bytes(int m, int n);
+cudaError_t float_alloc(FloatDev &d, int m, int n);
+void float_free(FloatDev &d);
+
+// Host-side table builders used when the caller passes NULL for a table (libm based).
+void build_sinc_table(int16_t *tab);   // returns false-free: table from the exact-rational recipe
+void build_twiddles_q15(int G, int16_t *tw2);   // [G/2][2]
+void build_hamming_q15(int len, int size, int32_t *out);
+
+}  // namespace pfa

@@ -1,0 +1,147 @@
+"""Host-side mirror of the reference's focusing interfaces, over the C ABI.
+
+* ``FixedPlan`` / ``form_image_fixed``: the datapath of ``silicon_emulator.form_image`` after the CPHD
+  read (mpfs/host/silicon_emulator.py:226-249), with its knobs ``grid``, ``range_sinc``, ``az_sinc``
+  (``--grid --range-sinc --az-sinc``; ``--deci`` is applied by ``prepare_tables``).  Returns the same
+  uint16 (grid, grid) image the emulator returns.
+* ``FloatPlan`` / ``focus_float``: ``form_image_pfa.pfa`` + detection (src/form_image_pfa.py:243-246,
+  mpfs/host/accel.py:39-44).
+
+Device memory and streams come from PyTorch; the arithmetic is entirely in libpfa_b200.so.  Tensors
+may be passed directly (CUDA tensors, no copy) or as NumPy arrays (copied in and out).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from . import geometry
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _stream_handle(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+class _Plan:
+    def __init__(self, cfg: _lib.Config):
+        self._lib = _lib.load()
+        h = C.c_void_p()
+        _lib.check(self._lib.pfa_plan_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.cfg = cfg
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def workspace_bytes(self) -> int:
+        return int(self._lib.pfa_plan_workspace_bytes(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.pfa_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class FixedPlan(_Plan):
+    """Bit-exact fixed-point frame former for an (m, n) scene on a (grid, grid) raster."""
+
+    def __init__(self, m: int, n: int, grid: int, range_sinc: bool = False, az_sinc: bool = False, device: int = 0):
+        cfg = _lib.Config(mode=_lib.MODE_FIXED, m=m, n=n, grid=grid,
+                          range_interp=_lib.SINC if range_sinc else _lib.LERP,
+                          az_interp=_lib.SINC if az_sinc else _lib.LERP, device=device)
+        super().__init__(cfg)
+        self.m, self.n, self.grid, self.device = m, n, grid, device
+
+    def set_tables(self, tables: dict):
+        """Upload the job derived from ``prepare_tables`` output (mpfs/host/sar_pipeline.py:36-115)."""
+        job = geometry.fixed_job(tables, self.grid)
+        return self.set_job(job)
+
+    def set_job(self, job: dict):
+        inv_order = np.empty(job["m"], np.int32)
+        inv_order[job["order"]] = np.arange(job["m"], dtype=np.int32)
+        keep = dict(f0=job["f0"], df=job["df"], pr=job["pr"], tan_s=job["tan_s"], inv_order=inv_order,
+                    kr=job["krp"], kc=job["kcp"], hr=np.ascontiguousarray(job["hamr"], np.int32),
+                    hc=np.ascontiguousarray(job["hamc"], np.int32),
+                    tw=np.ascontiguousarray(job["twiddle"], np.int16))
+        fj = _lib.FixedJob(_ptr(keep["f0"]), _ptr(keep["df"]), _ptr(keep["pr"]), _ptr(keep["tan_s"]),
+                           _ptr(keep["inv_order"]), _ptr(keep["kr"]), _ptr(keep["kc"]), _ptr(keep["hr"]),
+                           _ptr(keep["hc"]), _ptr(keep["tw"]), None)
+        _lib.check(self._lib.pfa_set_fixed_job(self._h, C.byref(fj)), self._h)
+        self._job = keep
+
+    def form(self, signal, out=None, stream=None):
+        """signal: (m, n) complex64 CUDA tensor (or NumPy array).  Returns a uint16 (grid, grid) image
+        [range bin][cross bin] -- a CUDA tensor for tensor input, a NumPy array for NumPy input."""
+        torch = _torch()
+        host = isinstance(signal, np.ndarray)
+        sig = torch.from_numpy(np.ascontiguousarray(signal, np.complex64)).to(f"cuda:{self.device}") if host \
+            else signal.contiguous()
+        if sig.dtype != torch.complex64 or tuple(sig.shape) != (self.m, self.n):
+            raise ValueError(f"signal must be complex64 {(self.m, self.n)}, got {sig.dtype} {tuple(sig.shape)}")
+        img = out if out is not None else torch.empty((self.grid, self.grid), dtype=torch.uint16, device=sig.device)
+        _lib.check(self._lib.pfa_form_fixed(self._h, C.c_void_p(sig.data_ptr()), C.c_void_p(img.data_ptr()),
+                                            _stream_handle(stream)), self._h)
+        if host:
+            return img.cpu().numpy()
+        return img
+
+    def form_iq16(self, sig_iq, out=None, stream=None):
+        """sig_iq: (m, n, 2) int16 CUDA tensor (quantised I/Q, the board's sig.bin layout)."""
+        torch = _torch()
+        img = out if out is not None else torch.empty((self.grid, self.grid), dtype=torch.uint16, device=sig_iq.device)
+        _lib.check(self._lib.pfa_form_fixed_iq16(self._h, C.c_void_p(sig_iq.data_ptr()), C.c_void_p(img.data_ptr()),
+                                                 _stream_handle(stream)), self._h)
+        return img
+
+    def form_host(self, signal: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+        """End-to-end through host buffers (pfa_form_fixed_host): copy in, form, copy out, sync."""
+        sig = np.ascontiguousarray(signal, np.complex64)
+        img = out if out is not None else np.empty((self.grid, self.grid), np.uint16)
+        _lib.check(self._lib.pfa_form_fixed_host(self._h, _ptr(sig), _ptr(img)), self._h)
+        return img
+
+    def exponents(self):
+        """(e_range[n], e_az[grid], q0_exp) of the last frame (fft_pass_bfp's per-row exponents)."""
+        er = np.zeros(self.n, np.int32)
+        ea = np.zeros(self.grid, np.int32)
+        q0 = C.c_int32(0)
+        _lib.check(self._lib.pfa_get_fixed_exponents(self._h, _ptr(er), _ptr(ea), C.byref(q0)), self._h)
+        return er, ea, int(q0.value)
+
+
+def form_image_fixed(signal, tables, grid, range_sinc=False, az_sinc=False, device=0):
+    """Drop-in for the emulator datapath: ``img = form_image_fixed(signal, tables, grid, rs, az)``
+    replaces silicon_emulator.py:226-249 (Q0 quantise .. detect_fixed) and returns the same uint16
+    (grid, grid) image."""
+    m, n = tables["dims"] if "dims" in tables else np.asarray(signal).shape
+    with FixedPlan(m, n, grid, range_sinc, az_sinc, device) as plan:
+        plan.set_tables(tables)
+        return plan.form(signal)
