@@ -141,6 +141,14 @@ pfa_status pfa_get_fixed_exponents(pfa_plan *plan, int32_t *e_range, int32_t *e_
 pfa_status pfa_form_float(pfa_plan *plan, const float *sig_dev, void *out_dev, int32_t detect, void *stream);
 pfa_status pfa_form_float_host(pfa_plan *plan, const float *sig_host, void *out_host, int32_t detect);
 
+/* Per-stage device timing, the counterpart of the board's per-stage timestamps sar_stage_ts[]
+ * (sar_sequencer.c:235-238) and form_image_pfa.StepTimer (src/form_image_pfa.py:42-60).  When enabled,
+ * every form call records CUDA events between its kernels on the launching stream.
+ * pfa_get_stage_times synchronises and writes up to `cap` stage durations (ms) of the last frame and
+ * their names (comma separated) into names[names_len]; *count receives the number of stages. */
+pfa_status pfa_set_profiling(pfa_plan *plan, int32_t enable);
+pfa_status pfa_get_stage_times(pfa_plan *plan, float *ms, int32_t cap, int32_t *count, char *names, size_t names_len);
+
 /* Diagnostics. */
 const char *pfa_status_string(pfa_status st);
 pfa_status pfa_last_error(const pfa_plan *plan, char *buf, size_t len);

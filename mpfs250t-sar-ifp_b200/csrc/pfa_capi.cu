@@ -185,6 +185,7 @@ pfa_status pfa_plan_destroy(pfa_plan *p) {
         if (p->staging_in) cudaFree(p->staging_in);
         if (p->staging_out) cudaFree(p->staging_out);
         if (p->host_stream) cudaStreamDestroy(p->host_stream);
+        for (auto &ev : p->prof.ev) if (ev) cudaEventDestroy(ev);
     }
     delete p;
     return PFA_OK;
@@ -250,7 +251,7 @@ static pfa_status fixed_common(pfa_plan *p, const float *sig, const int16_t *iq,
     if (iq && (reinterpret_cast<uintptr_t>(iq) & 3)) return fail(p, PFA_ERR_BAD_ARG, "iq16 signal must be 4-byte aligned");
     DeviceGuard dg(p->device);
     cudaError_t e = pfa::fixed_form(p->fx, sig, reinterpret_cast<const uint32_t *>(iq), img,
-                                    reinterpret_cast<cudaStream_t>(stream));
+                                    reinterpret_cast<cudaStream_t>(stream), &p->prof);
     if (e != cudaSuccess) return cuda_fail(p, e, "fixed form");
     return PFA_OK;
 }
@@ -321,6 +322,42 @@ pfa_status pfa_get_fixed_exponents(pfa_plan *p, int32_t *e_range, int32_t *e_az,
             return cuda_fail(p, e, "exponents");
         *q0_exp = ctrl[3];
     }
+    return PFA_OK;
+}
+
+pfa_status pfa_set_profiling(pfa_plan *p, int32_t enable) {
+    if (!p) return PFA_ERR_BAD_ARG;
+    DeviceGuard dg(p->device);
+    if (enable) {
+        for (auto &ev : p->prof.ev) {
+            if (!ev) {
+                cudaError_t e = cudaEventCreate(&ev);
+                if (e != cudaSuccess) return cuda_fail(p, e, "event create");
+            }
+        }
+    }
+    p->prof.on = enable != 0;
+    p->prof.count = 0;
+    return PFA_OK;
+}
+
+pfa_status pfa_get_stage_times(pfa_plan *p, float *ms, int32_t cap, int32_t *count, char *names, size_t names_len) {
+    if (!p || !count) return PFA_ERR_BAD_ARG;
+    DeviceGuard dg(p->device);
+    const int n = p->prof.count > 0 ? p->prof.count - 1 : 0;
+    *count = n;
+    std::string nm;
+    for (int i = 0; i < n; ++i) {
+        if (ms && i < cap) {
+            cudaError_t e = cudaEventSynchronize(p->prof.ev[i + 1]);
+            if (e != cudaSuccess) return cuda_fail(p, e, "event sync");
+            e = cudaEventElapsedTime(ms + i, p->prof.ev[i], p->prof.ev[i + 1]);
+            if (e != cudaSuccess) return cuda_fail(p, e, "event time");
+        }
+        if (i) nm += ",";
+        nm += p->prof.names[i + 1];
+    }
+    if (names && names_len) std::snprintf(names, names_len, "%s", nm.c_str());
     return PFA_OK;
 }
 

@@ -577,7 +577,7 @@ struct FixedLaunch {
     static size_t fft2_smem() { return 4 * (size_t)(N + N / 32) + 4 * (size_t)N + 2 * 32 * 4; }
 
     static cudaError_t run(const FixedDev &d, const float *sig, const uint32_t *sig_iq, uint16_t *img,
-                           cudaStream_t st) {
+                           cudaStream_t st, StageProf &pf) {
         cudaError_t e;
         // K0: Q0 block exponent
         if (sig) {
@@ -588,6 +588,7 @@ struct FixedLaunch {
                                              reinterpret_cast<uint32_t *>(d.ctrl));
             k_q0exp<<<1, 1, 0, st>>>(d.ctrl);
         }
+        if ((e = pf.mark(st, "q0max")) != cudaSuccess) return e;
         // K1: pass 1
         Pass1Args p1{reinterpret_cast<const float2 *>(sig), sig_iq, d.f0, d.df, d.fac, d.krp, d.order, d.sinc,
                      d.ctrl, d.p1, d.m, d.n, d.mpad};
@@ -601,6 +602,7 @@ struct FixedLaunch {
             if (e != cudaSuccess) return e;
             k_fx_pass1<false><<<g1, 256, p1_smem(false), st>>>(p1);
         }
+        if ((e = pf.mark(st, "pass1")) != cudaSuccess) return e;
         // K2: pass 2 + window + FFT-1
         Pass2Args p2{d.p1, d.tan_s, d.krp, d.kcp, d.hamr, d.hamc, d.tw, d.sinc, d.y1, d.e1, d.ctrl, d.m, d.n, d.mpad};
         const size_t s2 = pass2_smem(d.m, d.az_sinc != 0);
@@ -613,15 +615,18 @@ struct FixedLaunch {
             if (e != cudaSuccess) return e;
             k_fx_pass2_fft<L, E, false><<<d.n, T, s2, st>>>(p2);
         }
+        if ((e = pf.mark(st, "pass2_win_fft1")) != cudaSuccess) return e;
         // K3: FFT-2 along range
         Fft2Args f2{d.y1, d.e1, d.tw, d.y2, d.e2, d.ctrl, d.n};
         const size_t s3 = fft2_smem();
         e = cudaFuncSetAttribute(k_fx_fft2<L, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3);
         if (e != cudaSuccess) return e;
         k_fx_fft2<L, E><<<N, T, s3, st>>>(f2);
+        if ((e = pf.mark(st, "fft2")) != cudaSuccess) return e;
         // K4: renorm + detect + transpose
         dim3 g4(N / 64, N / 64);
         k_fx_detect<<<g4, 256, 0, st>>>(d.y2, d.e2, d.ctrl, img, N);
+        if ((e = pf.mark(st, "renorm_detect")) != cudaSuccess) return e;
         return cudaGetLastError();
     }
 };
@@ -629,20 +634,25 @@ struct FixedLaunch {
 }  // namespace
 
 cudaError_t fixed_form(const FixedDev &d, const float *sig_c64, const uint32_t *sig_iq, uint16_t *img,
-                       cudaStream_t st) {
+                       cudaStream_t st, StageProf *prof) {
+    StageProf none;
+    StageProf &pf = prof ? *prof : none;
+    pf.count = 0;
+    cudaError_t e = pf.mark(st, "start");
+    if (e != cudaSuccess) return e;
     // reset the reduction words: q0 max, emax1, emax2
-    cudaError_t e = cudaMemsetAsync(d.ctrl, 0, 4 * sizeof(int32_t), st);
+    e = cudaMemsetAsync(d.ctrl, 0, 4 * sizeof(int32_t), st);
     if (e != cudaSuccess) return e;
     switch (d.L) {
-        case 6: return FixedLaunch<6>::run(d, sig_c64, sig_iq, img, st);
-        case 7: return FixedLaunch<7>::run(d, sig_c64, sig_iq, img, st);
-        case 8: return FixedLaunch<8>::run(d, sig_c64, sig_iq, img, st);
-        case 9: return FixedLaunch<9>::run(d, sig_c64, sig_iq, img, st);
-        case 10: return FixedLaunch<10>::run(d, sig_c64, sig_iq, img, st);
-        case 11: return FixedLaunch<11>::run(d, sig_c64, sig_iq, img, st);
-        case 12: return FixedLaunch<12>::run(d, sig_c64, sig_iq, img, st);
-        case 13: return FixedLaunch<13>::run(d, sig_c64, sig_iq, img, st);
-        case 14: return FixedLaunch<14>::run(d, sig_c64, sig_iq, img, st);
+        case 6: return FixedLaunch<6>::run(d, sig_c64, sig_iq, img, st, pf);
+        case 7: return FixedLaunch<7>::run(d, sig_c64, sig_iq, img, st, pf);
+        case 8: return FixedLaunch<8>::run(d, sig_c64, sig_iq, img, st, pf);
+        case 9: return FixedLaunch<9>::run(d, sig_c64, sig_iq, img, st, pf);
+        case 10: return FixedLaunch<10>::run(d, sig_c64, sig_iq, img, st, pf);
+        case 11: return FixedLaunch<11>::run(d, sig_c64, sig_iq, img, st, pf);
+        case 12: return FixedLaunch<12>::run(d, sig_c64, sig_iq, img, st, pf);
+        case 13: return FixedLaunch<13>::run(d, sig_c64, sig_iq, img, st, pf);
+        case 14: return FixedLaunch<14>::run(d, sig_c64, sig_iq, img, st, pf);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -7,7 +7,7 @@ namespace pfa {
 size_t float_workspace_bytes(int, int) { return 0; }
 cudaError_t float_alloc(FloatDev &, int, int) { return cudaErrorInvalidValue; }
 void float_free(FloatDev &) {}
-cudaError_t float_form(const FloatDev &, const float2 *, void *, int, cudaStream_t) { return cudaErrorNotSupported; }
+cudaError_t float_form(const FloatDev &, const float2 *, void *, int, cudaStream_t, StageProf *) { return cudaErrorNotSupported; }
 }  // namespace pfa
 
 extern "C" {

@@ -47,6 +47,22 @@ struct FloatDev {
 
 }  // namespace pfa
 
+namespace pfa {
+// Stage events recorded between kernels when profiling is on.
+struct StageProf {
+    static constexpr int kMax = 12;
+    bool on = false;
+    int count = 0;                      // events recorded in the last frame
+    cudaEvent_t ev[kMax] = {};
+    const char *names[kMax] = {};
+    cudaError_t mark(cudaStream_t st, const char *name) {
+        if (!on || count >= kMax) return cudaSuccess;
+        names[count] = name;
+        return cudaEventRecord(ev[count++], st);
+    }
+};
+}  // namespace pfa
+
 struct pfa_plan {
     pfa_config cfg{};
     int device = 0;
@@ -58,6 +74,7 @@ struct pfa_plan {
     void *staging_out = nullptr;
     size_t staging_in_bytes = 0, staging_out_bytes = 0;
     cudaStream_t host_stream = nullptr;
+    pfa::StageProf prof;
     std::string err;
 };
 
@@ -65,12 +82,13 @@ namespace pfa {
 
 // Kernel launchers (pfa_fixed.cu / pfa_float.cu). They return a cudaError_t from the launches.
 cudaError_t fixed_form(const FixedDev &d, const float *sig_c64, const uint32_t *sig_iq, uint16_t *img,
-                       cudaStream_t st);
+                       cudaStream_t st, StageProf *prof);
 size_t fixed_workspace_bytes(int m, int n, int G);
 cudaError_t fixed_alloc(FixedDev &d, int m, int n, int G);
 void fixed_free(FixedDev &d);
 
-cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int detect, cudaStream_t st);
+cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int detect, cudaStream_t st,
+                       StageProf *prof);
 size_t float_workspace_bytes(int m, int n);
 cudaError_t float_alloc(FloatDev &d, int m, int n);
 void float_free(FloatDev &d);

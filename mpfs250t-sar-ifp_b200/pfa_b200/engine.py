@@ -51,6 +51,18 @@ class _Plan:
     def workspace_bytes(self) -> int:
         return int(self._lib.pfa_plan_workspace_bytes(self._h))
 
+    def set_profiling(self, enable: bool = True):
+        _lib.check(self._lib.pfa_set_profiling(self._h, 1 if enable else 0), self._h)
+
+    def stage_times(self) -> dict:
+        """{stage name: ms} of the last frame (needs set_profiling(True) before the frame)."""
+        ms = (C.c_float * 16)()
+        cnt = C.c_int32(0)
+        names = C.create_string_buffer(512)
+        _lib.check(self._lib.pfa_get_stage_times(self._h, ms, 16, C.byref(cnt), names, 512), self._h)
+        keys = names.value.decode().split(",") if cnt.value else []
+        return {k: float(ms[i]) for i, k in enumerate(keys)}
+
     def close(self):
         if getattr(self, "_h", None):
             self._lib.pfa_plan_destroy(self._h)

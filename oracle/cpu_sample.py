@@ -1,0 +1,133 @@
+"""ORACLE timing harness (used only by bench.py's cpu_baseline leg and its reference arm).
+
+Times the CPU restatement of the reference's fixed-point datapath (``fixed_emulator``, which follows
+mpfs/host/silicon_emulator.py line for line) on a bounded, evenly spaced sample of the lines of every
+stage of one frame, and scales each stage to the full frame:
+
+  Q0 quantise      whole signal (cheap)
+  pass 1           S of the m pulses                 -> x m/S
+  pass 2 + window  S of the G range rows             -> x G/S   (the emulator loops over all G rows)
+  FFT-1            S of the G rows (13 BFP stages)   -> x G/S
+  FFT-2            S of the G columns                -> x G/S
+  detect           S of the G rows                   -> x G/S
+
+The sampled lines are split over ``workers`` spawned processes (one chunk each) when workers > 1.
+"""
+from __future__ import annotations
+
+import os
+import time
+from concurrent.futures import ProcessPoolExecutor
+import multiprocessing as mp
+
+import numpy as np
+
+from . import fixed_emulator as fe
+
+
+def _pass1_chunk(args):
+    sr, si, geo, rows, sinc = args          # sr/si hold only the sampled pulses, in `rows` order
+    t = time.perf_counter()
+    n = geo["n"]
+    for r, i in enumerate(rows):
+        idx, wq = fe.bracket_q15(geo["KRp"], fe.pass1_coords(geo, i))
+        if sinc:
+            fe.gather_sinc(sr[r], si[r], idx, wq, n)
+        else:
+            fe.gather_lerp(sr[r], si[r], idx, wq, f32_product=True)
+    return time.perf_counter() - t
+
+
+def _pass2_chunk(args):
+    rowr, rowi, geo, rows, sinc = args
+    t = time.perf_counter()
+    m, G = geo["m"], geo["grid"]
+    hr = fe.hamming_q15(geo["n"], G)
+    hc = fe.hamming_q15(m, G)
+    for j in rows:
+        src = geo["KRp"][j] * geo["tan_s"]
+        idx, wq = fe.bracket_q15(geo["KCp"], src)
+        if sinc:
+            r, i = fe.gather_sinc(rowr, rowi, idx, wq, m)
+        else:
+            r, i = fe.gather_lerp(rowr, rowi, idx, wq)
+        cw = fe.wrap16((hr[j] * hc) >> 15)
+        fe.sat16(fe.wrap16((r * cw) >> 15))
+        fe.sat16(fe.wrap16((i * cw) >> 15))
+    return time.perf_counter() - t
+
+
+def _fft_chunk(args):
+    xr, xi = args
+    t = time.perf_counter()
+    fe.fft_bfp_rows(xr, xi)
+    return time.perf_counter() - t
+
+
+def _detect_chunk(args):
+    xr, xi = args
+    t = time.perf_counter()
+    fe.detect_q(xr, xi)
+    return time.perf_counter() - t
+
+
+def make_pool(workers: int):
+    """Spawned worker pool for fixed_frame_estimate (reuse it across calls)."""
+    return ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn"))
+
+
+def fixed_frame_estimate(signal, tables, grid, range_sinc=True, az_sinc=True, sample=64, workers=1, seed=0,
+                         pool=None):
+    """Estimated single-frame time (ms) of the oracle, from `sample` lines per stage."""
+    rng = np.random.default_rng(seed)
+    stage = {}
+    t = time.perf_counter()
+    sr, si, _ = fe.quantize_q0(np.asarray(signal, np.complex64))
+    stage["q0"] = time.perf_counter() - t
+    geo = fe.fixed_geometry(tables, grid)
+    m, n, G = geo["m"], geo["n"], grid
+    s1 = min(sample, m)
+    s2 = min(sample, G)
+    p1_rows = np.linspace(0, m - 1, s1).astype(int)
+    p2_rows = np.linspace(0, n - 1, s2).astype(int)
+    # representative pass-2 source row and FFT operands (timing does not depend on the values)
+    rowr = rng.integers(-2000, 2000, m).astype(np.int64)
+    rowi = rng.integers(-2000, 2000, m).astype(np.int64)
+    fr = rng.integers(-2000, 2000, (s2, G)).astype(np.int64)
+    fi = rng.integers(-2000, 2000, (s2, G)).astype(np.int64)
+
+    def split(rows):
+        return [c for c in np.array_split(rows, workers) if len(c)]
+
+    own = False
+    if workers > 1:
+        ex = pool
+        if ex is None:
+            ex, own = make_pool(workers), True
+        run = lambda fn, jobs: max(ex.map(fn, jobs)) if jobs else 0.0   # noqa: E731
+    else:
+        ex = None
+        run = lambda fn, jobs: sum(map(fn, jobs))                          # noqa: E731
+    try:
+        if ex is not None:          # warm the workers (imports) outside the timed stages
+            list(ex.map(_fft_chunk, [(fr[:1, :64], fi[:1, :64])] * workers))
+        stage["pass1"] = run(_pass1_chunk, [(sr[c], si[c], geo, c, range_sinc) for c in split(p1_rows)]) * m / s1
+        stage["pass2_window"] = run(_pass2_chunk, [(rowr, rowi, geo, c, az_sinc) for c in split(p2_rows)]) * G / s2
+        fc = [(fr[c], fi[c]) for c in split(np.arange(s2))]
+        stage["fft1"] = run(_fft_chunk, fc) * G / s2
+        stage["fft2"] = run(_fft_chunk, fc) * G / s2
+        stage["detect"] = run(_detect_chunk, fc) * G / s2
+    finally:
+        if own:
+            ex.shutdown()
+    total = sum(stage.values())
+    return dict(ms_per_frame=1000.0 * total, stage_seconds={k: round(v, 4) for k, v in stage.items()},
+                sample=f"{s1} of {m} pulses, {s2} of {G} rows/columns per FFT/resample stage, "
+                       f"scaled to the full frame", workers=workers)
+
+
+def available_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
