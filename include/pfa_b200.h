@@ -42,7 +42,8 @@ typedef enum pfa_status {
     PFA_ERR_CUDA = 5,         /* CUDA runtime error (message in pfa_last_error)                  */
     PFA_ERR_ALLOC = 6,        /* device allocation failed                                        */
     PFA_ERR_TIMEOUT = 7,      /* a bounded wait ran out                                          */
-    PFA_ERR_NO_DEVICE = 8     /* no usable sm_100 device                                         */
+    PFA_ERR_NO_DEVICE = 8,    /* no usable sm_100 device                                         */
+    PFA_ERR_TOO_LARGE = 9     /* frame larger than pfa_form_fixed_noalloc's static scratch allows */
 } pfa_status;
 
 enum pfa_mode { PFA_MODE_FIXED = 0, PFA_MODE_FLOAT32 = 1, PFA_MODE_MIXED = 2 };
@@ -129,6 +130,23 @@ pfa_status pfa_form_fixed(pfa_plan *plan, const float *sig_dev, uint16_t *img_de
 pfa_status pfa_form_fixed_iq16(pfa_plan *plan, const int16_t *sig_iq_dev, uint16_t *img_dev, void *stream);
 /* End-to-end host variant: copies the host signal in, forms, copies the image out, synchronises. */
 pfa_status pfa_form_fixed_host(pfa_plan *plan, const float *sig_host, uint16_t *img_host);
+
+/* Allocation-free fixed-point frame, for callers that cannot allocate device memory: code running
+ * where cudaMalloc is forbidden or unsafe (inside a host that owns all device memory through its own
+ * pool, a real-time loop that must not hit the allocator, or a process whose allocator is already
+ * exhausted).  No counterpart in the reference (its board code uses fixed DDR buffers and never
+ * allocates; this mirrors that property rather than any one function).
+ * Everything the frame needs besides the caller's signal and image -- the job vectors and the three
+ * intermediate frames -- lives in one file-scope static __device__ array of 12.1 MB that every GPU
+ * which loads the library holds until the process exits.  Limits: grid <= 1024, m <= grid, n <= grid,
+ * otherwise PFA_ERR_TOO_LARGE.  job must carry ham_r, ham_c and twiddle (no host-side table building);
+ * sinc_q15 may be NULL (built-in table).  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call before any stream capture.
+ * All calls share the one array and it keeps the last call's contents: calls that overlap on the GPU
+ * (different streams, threads or processes sharing a context) race and corrupt each other; serialise
+ * them.  Calls no allocating routine: no cudaMalloc/cudaFree, no host heap. */
+pfa_status pfa_form_fixed_noalloc(const pfa_config *cfg, const pfa_fixed_job *job, const float *sig_dev,
+                                  uint16_t *img_dev, void *stream);
 
 /* Per-row BFP exponents of the last fixed frame (silicon_emulator.fft_pass_bfp's `e`, :198-205):
  * e_range[n] (FFT-1 rows = range bins < n; rows >= n are all-zero and have exponent 0),

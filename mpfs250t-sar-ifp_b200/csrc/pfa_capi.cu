@@ -15,6 +15,7 @@ namespace pfa {
 #include "gen/sinc_q15.inc"   // kSincQ15[256 * 32], generated at build time by the exact-rational recipe
 
 void build_sinc_table(int16_t *tab) { std::memcpy(tab, kSincQ15, sizeof(kSincQ15)); }
+const int16_t *builtin_sinc_table() { return kSincQ15; }
 
 void build_twiddles_q15(int G, int16_t *tw2) {
     // floor(exp(-2 pi j k / G) * 32768) clipped to int16 (src/fixedpoint.py:277, quant mode 'trunc')
@@ -122,6 +123,7 @@ const char *pfa_status_string(pfa_status st) {
         case PFA_ERR_ALLOC: return "device allocation failed";
         case PFA_ERR_TIMEOUT: return "timeout";
         case PFA_ERR_NO_DEVICE: return "no usable device";
+        case PFA_ERR_TOO_LARGE: return "frame exceeds the no-allocation entry point's static scratch (grid <= 1024)";
     }
     return "unknown status";
 }

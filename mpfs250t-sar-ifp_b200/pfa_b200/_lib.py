@@ -11,7 +11,7 @@ from pathlib import Path
 
 LIB_PATH = Path(os.environ.get("PFA_B200_LIB", Path(__file__).resolve().parent / "lib" / "libpfa_b200.so"))
 
-OK, BAD_CONFIG, BAD_DIMS, BAD_ARG, NOT_READY, CUDA, ALLOC, TIMEOUT, NO_DEVICE = range(9)
+OK, BAD_CONFIG, BAD_DIMS, BAD_ARG, NOT_READY, CUDA, ALLOC, TIMEOUT, NO_DEVICE, TOO_LARGE = range(10)
 MODE_FIXED, MODE_FLOAT32, MODE_MIXED = 0, 1, 2
 LERP, SINC = 0, 1
 LAYOUT_CENTRED, LAYOUT_NATURAL = 0, 1
@@ -58,6 +58,8 @@ SIGNATURES = {
     "pfa_form_fixed_iq16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "pfa_form_fixed_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "pfa_get_fixed_exponents": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pfa_form_fixed_noalloc": (C.c_int, [C.POINTER(Config), C.POINTER(FixedJob), C.c_void_p, C.c_void_p,
+                                         C.c_void_p]),
     "pfa_form_float": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "pfa_form_float_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
     "pfa_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
