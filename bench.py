@@ -37,10 +37,16 @@ METRIC = "ms per 8192^2 PFA frame (mixed vs FP32 at stated err vs FP64); autofoc
 FPGA_FRAME_MS = {"centerfield_5634x4319": 14170.0, "ndsu_8167x8192": 15738.0}   # BASELINE.md (MPFS250T fabric)
 
 WORKLOADS = {
-    "centerfield_5634x4319": dict(mode="fixed", grid=8192, range_sinc=True, az_sinc=True,
+    "centerfield_5634x4319": dict(mode="fixed", grid=8192, range_sinc=True, az_sinc=True, scene="centerfield_5634x4319",
                                   desc="Centerfield-shaped 5634x4319 c64 -> 8192^2, fixed point, "
                                        "--deci 1 --grid 8192 --range-sinc --az-sinc, 256 targets + "
                                        "Rayleigh clutter -10 dB, seed 2"),
+    "ndsu_8167x8192_fp32": dict(mode="float", mixed=False, range_sinc=False, az_sinc=False, scene="ndsu_8167x8192",
+                                desc="NDSU-shaped 8167x8192 c64 -> 8192^2, float FP32 (lerp, form_image_pfa), "
+                                     "1024 targets + Rayleigh clutter -10 dB, 15 dB SNR, seed 3"),
+    "ndsu_8167x8192_fp32_sinc": dict(mode="float", mixed=False, range_sinc=True, az_sinc=True, scene="ndsu_8167x8192",
+                                     desc="NDSU-shaped 8167x8192 c64 -> 8192^2, float FP32, 32-tap sinc both passes, "
+                                          "1024 targets + Rayleigh clutter -10 dB, 15 dB SNR, seed 3"),
 }
 
 
@@ -128,9 +134,15 @@ def _traffic(kernel: str, workload: str):
     return None
 
 
-def stage_bytes(stage: str, m: int, n: int, G: int) -> float:
-    """Algorithmic (compulsory) HBM bytes per launch of each fixed-point kernel."""
+def stage_bytes(stage: str, m: int, n: int, G: int, mode: str = "fixed") -> float:
+    """Algorithmic (compulsory) HBM bytes per launch of each kernel (G = pow2 raster side)."""
     mpad = (m + 31) // 32 * 32
+    if mode == "float":
+        return {
+            "pass1": 8.0 * m * n + 8.0 * n * mpad,          # read c64 signal, write c64 range-bin rows
+            "pass2_win_fft1": 8.0 * n * mpad + 8.0 * n * G,  # read rows, write cross-FFT rows
+            "fft2_detect": 8.0 * n * G + 4.0 * G * G,        # read cross-FFT columns, write f32 |img|
+        }[stage]
     return {
         "q0max": 8.0 * m * n,                              # read the complex64 signal
         "pass1": 8.0 * m * n + 4.0 * n * mpad,             # read signal, write int16x2 range-bin rows
@@ -152,15 +164,25 @@ def run_ours(a, ws, rank, local):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
     wl = WORKLOADS[a.workload]
-    sc = synth.workload_scene(a.workload)
+    mode = wl["mode"]
+    sc = synth.workload_scene(wl["scene"])
     m, n = sc.signal.shape
-    G = wl["grid"]
     tables = geometry.prepare_tables_from_scene(sc)
     sig_host = torch.from_numpy(sc.signal).pin_memory()
     sig = sig_host.to(dev)
-    plan = engine.FixedPlan(m, n, G, wl["range_sinc"], wl["az_sinc"], device=local)
+    if mode == "fixed":
+        G = wl["grid"]
+        plan = engine.FixedPlan(m, n, G, wl["range_sinc"], wl["az_sinc"], device=local)
+        img = torch.empty((G, G), dtype=torch.uint16, device=dev)
+        out_bytes = G * G * 2
+        launches_per_frame = 6
+    else:
+        G = geometry.pow2(max(m, n))
+        plan = engine.FloatPlan(m, n, wl["range_sinc"], wl["az_sinc"], wl.get("mixed", False), device=local)
+        img = torch.empty((plan.m2, plan.n2), dtype=torch.float32, device=dev)
+        out_bytes = plan.m2 * plan.n2 * 4
+        launches_per_frame = 3
     plan.set_tables(tables)
-    img = torch.empty((G, G), dtype=torch.uint16, device=dev)
     stream = torch.cuda.current_stream()
 
     def barrier():
@@ -205,13 +227,15 @@ def run_ours(a, ws, rank, local):
     stages = {k: statistics.mean(v) for k, v in acc.items()}
     top = max(stages, key=stages.get)
     hbm, peak_kind = _peaks()
-    ach = stage_bytes(top, m, n, G) / (stages[top] * 1e-3) / 1e9
-    traffic = _traffic({"pass1": "k_fx_pass1", "pass2_win_fft1": "k_fx_pass2_fft", "fft2": "k_fx_fft2",
-                        "renorm_detect": "k_fx_detect", "q0max": "k_q0max"}[top], a.workload)
-    frame_bytes = sum(stage_bytes(s, m, n, G) for s in stages)
+    ach = stage_bytes(top, m, n, G, mode) / (stages[top] * 1e-3) / 1e9
+    kname = ({"pass1": "k_fx_pass1", "pass2_win_fft1": "k_fx_pass2_fft", "fft2": "k_fx_fft2",
+              "renorm_detect": "k_fx_detect", "q0max": "k_q0max"} if mode == "fixed" else
+             {"pass1": "k_fl_pass1", "pass2_win_fft1": "k_fl_pass2_fft", "fft2_detect": "k_fl_fft2"})[top]
+    traffic = _traffic(kname, a.workload)
+    frame_bytes = sum(stage_bytes(s, m, n, G, mode) for s in stages)
 
     # ---- end to end through the host-buffer C-ABI entry point (pinned host in/out)
-    img_host = torch.empty((G, G), dtype=torch.uint16).pin_memory()
+    img_host = torch.empty(tuple(img.shape), dtype=img.dtype).pin_memory()
     sig_np = sig_host.numpy()
     img_np = img_host.numpy()
     for _ in range(2):
@@ -227,8 +251,11 @@ def run_ours(a, ws, rank, local):
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         from oracle import cpu_sample
-        est = cpu_sample.fixed_frame_estimate(sc.signal, tables, G, wl["range_sinc"], wl["az_sinc"],
-                                              sample=a.cpu_sample, workers=1)
+        if mode == "fixed":
+            est = cpu_sample.fixed_frame_estimate(sc.signal, tables, G, wl["range_sinc"], wl["az_sinc"],
+                                                  sample=a.cpu_sample, workers=1)
+        else:
+            est = cpu_sample.float_frame_estimate(sc.signal, tables, sample=a.cpu_sample, workers=1)
         cpu = {"value": round(est["ms_per_frame"], 1), "unit": "ms/frame", "cores": 1, "kind": "port",
                "sample": est["sample"], "stage_seconds": est["stage_seconds"]}
 
@@ -237,19 +264,22 @@ def run_ours(a, ws, rank, local):
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(dev_ms / a.steps, 4),
         "higher_is_better": False, "scaling": "weak",
         "vs_baseline": round(ms_per_frame / FPGA_FRAME_MS[a.workload], 8) if a.workload in FPGA_FRAME_MS else None,
-        "dtype": "int16 fixed point (int32/int64 accumulate; fp64 coordinates)", "data": "synthetic",
+        "dtype": ("int16 fixed point (int32/int64 accumulate; fp64 coordinates)" if mode == "fixed"
+                  else "fp32 (fp64 coordinates)"), "data": "synthetic",
         "config": {"workload": a.workload, "desc": wl["desc"], "m": m, "n": n, "grid": G,
-                   "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (195 MB signal, 268 MB FFT-2 buffer); no flush",
+                   "parallelism": f"replicas x{ws}",
+                   "l2": f"inputs larger than L2 ({sc.signal.nbytes / 1e6:.0f} MB signal, "
+                         f"{G * G * 4 / 1e6:.0f}+ MB intermediates); no flush",
                    "frames_per_s": round(1000.0 / ms_per_frame, 2)},
         "stages_ms": {k: round(v, 4) for k, v in stages.items()},
-        "roofline": {"kernel": top, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                     "frac": round(ach / hbm, 4), "peak_kind": f"of {peak_kind}",
-                     "traffic": traffic, "algorithmic_bytes": stage_bytes(top, m, n, G),
+        "roofline": {"kernel": kname, "stage": top, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm,
+                     "unit": "GB/s", "frac": round(ach / hbm, 4), "peak_kind": f"of {peak_kind}",
+                     "traffic": traffic, "algorithmic_bytes": stage_bytes(top, m, n, G, mode),
                      "frame_bytes": frame_bytes,
                      "frame_frac": round(frame_bytes / (ms_per_frame * 1e-3) / 1e9 / hbm, 4)},
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms/frame", "h2d_bytes_per_step": int(sc.signal.nbytes),
-                "d2h_bytes_per_step": int(G * G * 2)},
-        "gpu_launches": 6 * a.steps,
+                "d2h_bytes_per_step": int(out_bytes)},
+        "gpu_launches": launches_per_frame * a.steps,
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
@@ -267,17 +297,21 @@ def run_reference(a, ws, rank):
     from pfa_b200 import geometry, synth
     from oracle import cpu_sample
     wl = WORKLOADS[a.workload]
-    sc = synth.workload_scene(a.workload)
+    sc = synth.workload_scene(wl["scene"])
     m, n = sc.signal.shape
-    G = wl["grid"]
+    G = wl.get("grid", geometry.pow2(max(m, n)))
     tables = geometry.prepare_tables_from_scene(sc)
     cores = cpu_sample.available_cores()
     per = []
     pool = cpu_sample.make_pool(cores) if cores > 1 else None
     try:
         for i in range(a.warmup + a.steps):
-            est = cpu_sample.fixed_frame_estimate(sc.signal, tables, G, wl["range_sinc"], wl["az_sinc"],
-                                                  sample=a.ref_sample, workers=cores, seed=i, pool=pool)
+            if wl["mode"] == "fixed":
+                est = cpu_sample.fixed_frame_estimate(sc.signal, tables, G, wl["range_sinc"], wl["az_sinc"],
+                                                      sample=a.ref_sample, workers=cores, seed=i, pool=pool)
+            else:
+                est = cpu_sample.float_frame_estimate(sc.signal, tables, sample=a.ref_sample, workers=cores,
+                                                      seed=i, pool=pool)
             if i >= a.warmup:
                 per.append(est["ms_per_frame"])
     finally:
@@ -288,7 +322,8 @@ def run_reference(a, ws, rank):
         "metric": METRIC, "value": round(v, 1), "unit": "ms/frame", "n_gpus": ws, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(v, 1), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": round(v / FPGA_FRAME_MS[a.workload], 6) if a.workload in FPGA_FRAME_MS else None,
-        "dtype": "int16 fixed point (int64 numpy)", "data": "synthetic", "impl": "reference",
+        "dtype": "int16 fixed point (int64 numpy)" if wl["mode"] == "fixed" else "complex64/float64 numpy",
+        "data": "synthetic", "impl": "reference",
         "config": {"workload": a.workload, "desc": wl["desc"], "m": m, "n": n, "grid": G},
         "cpu_baseline": {"value": round(v, 1), "unit": "ms/frame", "cores": cores, "kind": "port",
                          "sample": est["sample"] + f"; {cores} spawned worker processes"},

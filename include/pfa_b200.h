@@ -93,8 +93,11 @@ typedef struct pfa_fixed_job {
 /* Float job: host pointers, copied at pfa_set_float_job.  Mirrors form_image_pfa.resample_kspace
  * (src/form_image_pfa.py:177-217); freq[i,k] = f0[i] + k*df[i]. */
 typedef struct pfa_float_job {
-    const double *f0;         /* [m] */
-    const double *df;         /* [m] */
+    const double *f0;         /* [m] freq[:, 0]                                                   */
+    const double *df;         /* [m] frequency step along the pulse                               */
+    const double *f_last;     /* [m] freq[:, n-1]: the end points' wavenumbers (2 f / c) pr are
+                                 evaluated exactly as the reference does, since the output grid
+                                 KR starts and ends exactly on one pulse's end points               */
     const double *pr;         /* [m] radial projection                                          */
     const double *tan_s;      /* [m] tan(phi) sorted ascending                                   */
     const int32_t *order;     /* [m] argsort(tan_phi)                                            */

@@ -1,17 +1,618 @@
-// Float PFA datapath (FP32 and split-precision) -- placeholder until the float kernels land.
+// Float PFA datapath on sm_100a: the drop-in for form_image_pfa.pfa + detection
+// (src/form_image_pfa.py:165-246, mpfs/host/accel.py:39-44).
+//
+//   k_fl_pass1      per pulse: FP64 source wavenumbers kr = (2 freq / c) pr, np.interp bracket
+//                   (xp[j] <= x < xp[j+1], zero outside [xp0, xp_last]), FP32 lerp (or the float sinc
+//                   variant); 32-slot x 128-bin shared tile -> range-bin rows of tan(phi)-sorted pulses
+//   k_fl_pass2_fft  per range bin j: source KR[j] * tan_s (FP64), bracket, gather, float32 Hamming
+//                   product window, (-1)^(j+k) centring modulation, FP32 FFT along cross (length m2)
+//   k_fl_fft2       per cross bin: FP32 FFT along range (length n2, rows j >= n are the zero pad),
+//                   fused detection store (|z|, |z|^2 or complex with the (-1)^(u+v) centring sign)
+//
+// Centring: fftshift(fft(ifftshift(x)))[v] = (-1)^v fft((-1)^a x[a])[v] for even N with N/2 even, so the
+// shifts of form_image_pfa.transform2d (:144-147) cost one sign flip on load and one on store.
 #include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
 
 #include "pfa_internal.h"
 
 namespace pfa {
-size_t float_workspace_bytes(int, int) { return 0; }
-cudaError_t float_alloc(FloatDev &, int, int) { return cudaErrorInvalidValue; }
-void float_free(FloatDev &) {}
-cudaError_t float_form(const FloatDev &, const float2 *, void *, int, cudaStream_t, StageProf *) { return cudaErrorNotSupported; }
+const int16_t *builtin_sinc_table();
+
+namespace {
+
+constexpr double kC = 299792458.0;
+
+// ------------------------------------------------------------------------------------------ FFT
+// Radix-2 DIT FFT in registers (E complex values per thread, T = N/E threads), bit groups of LE
+// stages between shared-memory exchanges -- the same thread/position mapping as the fixed-point
+// transform.  Twiddles: stage-contiguous table (stage b: 2^b entries at offset 2^b - 1).
+template <int L, int E>
+struct F32Fft {
+    static constexpr int N = 1 << L;
+    static constexpr int LE = (E == 16) ? 4 : (E == 8) ? 3 : (E == 4) ? 2 : 1;
+    static constexpr int T = N / E;
+    static constexpr int TB = L - LE;
+    static constexpr int NG = (L + LE - 1) / LE;
+    static_assert(T >= 32, "at least one warp");
+
+    __device__ static __forceinline__ int group_lo(int g) { return (g * LE + LE <= L) ? g * LE : (L - LE); }
+    __device__ static __forceinline__ int pos(int lo, int t, int v) {
+        return (t & ((1 << lo) - 1)) | (v << lo) | ((t >> lo) << (lo + LE));
+    }
+    __device__ static __forceinline__ int swz(int p) { return p + (p >> 4); }
+    __device__ static __forceinline__ int logical(int g, int tid) {
+        return g == 0 ? (int)(__brev((unsigned)tid) >> (32 - TB)) : tid;
+    }
+    static constexpr int xbuf_elems() { return N + N / 16; }
+
+    // In: group-0 layout (element v of thread tid = natural index tid + T * bitrev(v)).
+    // Out: element v of thread tid = frequency index tid + T * v.
+    __device__ static void run(float2 (&x)[E], float2 *xbuf, const float2 *__restrict__ tw, int tid) {
+        int done = 0;
+#pragma unroll
+        for (int g = 0; g < NG; ++g) {
+            const int lo = group_lo(g);
+            const int t = logical(g, tid);
+            if (g > 0) {
+                const int plo = group_lo(g - 1);
+                const int pt = logical(g - 1, tid);
+                __syncthreads();
+#pragma unroll
+                for (int v = 0; v < E; ++v) xbuf[swz(pos(plo, pt, v))] = x[v];
+                __syncthreads();
+#pragma unroll
+                for (int v = 0; v < E; ++v) x[v] = xbuf[swz(pos(lo, t, v))];
+            }
+            const int tlow = t & ((1 << lo) - 1);
+#pragma unroll
+            for (int rb = 0; rb < LE; ++rb) {
+                const int b = lo + rb;
+                if (b < done) continue;
+                const float2 *tws = tw + ((1 << b) - 1);
+#pragma unroll
+                for (int v = 0; v < E; ++v) {
+                    if (v & (1 << rb)) continue;
+                    const int v2 = v | (1 << rb);
+                    const int k = tlow | ((v & ((1 << rb) - 1)) << lo);
+                    const float2 w = __ldg(tws + k);
+                    const float2 bb = x[v2];
+                    const float2 tt = make_float2(fmaf(w.x, bb.x, -w.y * bb.y), fmaf(w.x, bb.y, w.y * bb.x));
+                    const float2 a = x[v];
+                    x[v] = make_float2(a.x + tt.x, a.y + tt.y);
+                    x[v2] = make_float2(a.x - tt.x, a.y - tt.y);
+                }
+            }
+            done = lo + LE;
+        }
+    }
+};
+
+// ------------------------------------------------------------------------------------------ brackets
+// np.interp bracket on an ascending accessor xa(0..n-1): returns j with xa(j) <= x < xa(j+1) and the
+// fraction, or -1 when x is outside [xa(0), xa(n-1)]; x == xa(n-1) gives j = n-2, frac = 1.
+struct Frac {
+    float f;     // fraction toward the upper natural-order sample (lerp weight)
+    int ph;      // sinc phase round(frac * 32768) >> 7, taken from the float64 ascending fraction
+    int rev;     // descending source axis: taps run in reverse natural order
+};
+
+template <class F>
+__device__ __forceinline__ int interp_bracket(const F &xa, int n, double x0, double x1, double x, int guess, Frac &frac) {
+    if (!(x >= x0) || !(x <= x1)) return -1;
+    // largest j with xa(j) <= x
+    int j = min(max(guess, 0), n - 1);
+    int steps = 0;
+    while (j + 1 < n && xa(j + 1) <= x) {
+        ++j;
+        if (++steps > 6) {
+            int lo = j, hi = n - 1;          // xa(lo) <= x; find the last index with xa <= x
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (xa(mid) <= x) lo = mid; else hi = mid - 1;
+            }
+            j = lo;
+            break;
+        }
+    }
+    while (j > 0 && xa(j) > x) {
+        --j;
+        if (++steps > 12) {
+            int lo = 0, hi = j;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (xa(mid) <= x) lo = mid; else hi = mid - 1;
+            }
+            j = lo;
+            break;
+        }
+    }
+    if (j >= n - 1) j = n - 2;
+    const double a = xa(j), b = xa(j + 1);
+    const double fd = __ddiv_rn(__dsub_rn(x, a), __dsub_rn(b, a));
+    frac.f = (float)fd;
+    frac.ph = (int)fmin(rint(__dmul_rn(fd, 32768.0)), 32767.0) >> 7;
+    frac.rev = 0;
+    return j;
+}
+
+// the same bracket seen from the descending side: lower natural index n-2-j, weights mirrored
+__device__ __forceinline__ void mirror_frac(Frac &fr) {
+    fr.f = 1.0f - fr.f;
+    fr.rev = 1;
+}
+
+// lerp or float sinc of complex64 samples `src` (indexed from `base`) at bracket (j, frac)
+template <bool SINC>
+__device__ __forceinline__ float2 gather_f32(const float2 *src, int base, int sn, int j, Frac fr,
+                                             const float *tab) {
+    if (j < 0) return make_float2(0.f, 0.f);
+    const float frac = fr.f;
+    if (SINC && j >= 15 && j <= sn - 17) {
+        const float *c = tab + fr.ph * 32;
+        const float2 *x = src + (j - 15 - base);
+        float ar = 0.f, ai = 0.f;
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+            const float ct = fr.rev ? c[31 - t] : c[t];
+            ar = fmaf(ct, x[t].x, ar);
+            ai = fmaf(ct, x[t].y, ai);
+        }
+        return make_float2(ar, ai);
+    }
+    const float2 a = src[j - base], b = src[j + 1 - base];
+    return make_float2(fmaf(frac, b.x - a.x, a.x), fmaf(frac, b.y - a.y, a.y));
+}
+
+// ------------------------------------------------------------------------------------------ K1f
+constexpr int F1_SLOTS = 32, F1_BINS = 128, F1_WARPS = 8, F1_WMAX = 384;
+
+struct FPass1Args {
+    const float2 *sig;
+    const double *f0, *df, *flast, *pr, *kr_grid;
+    const int32_t *order;
+    const float *tabf;
+    float2 *p1;
+    int m, n, mpad;
+};
+
+constexpr size_t f1_smem(bool sinc) {
+    return (size_t)F1_BINS * (F1_SLOTS + 1) * 8 + (size_t)F1_WARPS * F1_WMAX * 8 + (sinc ? 256 * 32 * 4 : 0);
+}
+
+template <bool SINC>
+__global__ void __launch_bounds__(256) k_fl_pass1(FPass1Args a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2(*tile)[F1_SLOTS + 1] = reinterpret_cast<float2(*)[F1_SLOTS + 1]>(smem);
+    float2(*win)[F1_WMAX] = reinterpret_cast<float2(*)[F1_WMAX]>(smem + (size_t)F1_BINS * (F1_SLOTS + 1) * 8);
+    float *tab = reinterpret_cast<float *>(smem + (size_t)F1_BINS * (F1_SLOTS + 1) * 8 + (size_t)F1_WARPS * F1_WMAX * 8);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int r0 = blockIdx.x * F1_SLOTS, j0 = blockIdx.y * F1_BINS;
+    const int n = a.n;
+    if (SINC)
+        for (int i = tid; i < 256 * 32; i += blockDim.x) tab[i] = a.tabf[i];
+    __syncthreads();
+    for (int s = 0; s < F1_SLOTS / F1_WARPS; ++s) {
+        const int slot = warp + F1_WARPS * s;
+        const int r = r0 + slot;
+        if (r >= a.m) {
+            for (int t = lane; t < F1_BINS; t += 32) tile[t][slot] = make_float2(0.f, 0.f);
+            continue;
+        }
+        const int i = a.order[r];
+        const double f0 = a.f0[i], df = a.df[i], pri = a.pr[i], sc = 2.0 * pri / kC;
+        // kr[i, k] = (2 freq[i, k] / c) pr[i] (form_image_pfa.py:176-187).  The end points are evaluated
+        // with the reference's exact IEEE operations (KR's first and last samples coincide with some
+        // pulse's end points, where np.interp returns the end sample); interior samples use the affine
+        // model freq = f0 + k df.
+        const double kfirst = __dmul_rn(__ddiv_rn(__dmul_rn(2.0, f0), kC), pri);
+        const double klast = __dmul_rn(__ddiv_rn(__dmul_rn(2.0, a.flast[i]), kC), pri);
+        auto kr = [&](int k) { return k == 0 ? kfirst : (k == n - 1 ? klast : sc * (f0 + (double)k * df)); };
+        const bool asc = kr(n - 1) >= kr(0);
+        auto xa = [&](int t) { return asc ? kr(t) : kr(n - 1 - t); };
+        const double xa0 = xa(0), xa1 = xa(n - 1);
+        const double inv = 1.0 / (sc * df);
+        int jj[F1_BINS / 32];
+        Frac fr[F1_BINS / 32];
+        int lo_i = 1 << 30, hi_i = -1;
+#pragma unroll
+        for (int t = 0; t < F1_BINS / 32; ++t) {
+            const int j = j0 + lane + 32 * t;
+            jj[t] = -1;
+            fr[t] = Frac{0.f, 0, 0};
+            if (j < n) {
+                const double q = a.kr_grid[j];
+                const double kest = q * inv - f0 / df;
+                int g = 0;
+                if (isfinite(kest)) g = (int)fmin(fmax(asc ? floor(kest) : floor((double)(n - 1) - kest), 0.0), (double)(n - 1));
+                const int ja = interp_bracket(xa, n, xa0, xa1, q, g, fr[t]);
+                if (ja >= 0) {
+                    // natural-order index of the lower sample and the weight toward the upper one
+                    int lowi;
+                    if (asc) { lowi = ja; } else { lowi = n - 2 - ja; mirror_frac(fr[t]); }
+                    jj[t] = lowi;
+                    lo_i = min(lo_i, lowi);
+                    hi_i = max(hi_i, lowi);
+                }
+            }
+        }
+        lo_i = __reduce_min_sync(0xffffffffu, lo_i);
+        hi_i = __reduce_max_sync(0xffffffffu, hi_i);
+        int wlo = 0, whi = 0;
+        if (hi_i >= 0) {
+            wlo = max(0, lo_i - (SINC ? 15 : 0));
+            whi = min(n, hi_i + (SINC ? 17 : 2));
+        }
+        const bool fits = whi - wlo <= F1_WMAX;
+        float2 *w = win[warp];
+        const float2 *row = a.sig + (size_t)i * n;
+        if (fits)
+            for (int k = wlo + lane; k < whi; k += 32) w[k - wlo] = row[k];
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < F1_BINS / 32; ++t) {
+            const int jb = lane + 32 * t;
+            float2 out = make_float2(0.f, 0.f);
+            if (j0 + jb < n && jj[t] >= 0)
+                out = fits ? gather_f32<SINC>(w, wlo, n, jj[t], fr[t], tab) : gather_f32<SINC>(row, 0, n, jj[t], fr[t], tab);
+            tile[jb][slot] = out;
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int jb = warp; jb < F1_BINS; jb += F1_WARPS) {
+        const int j = j0 + jb;
+        if (j >= n) break;
+        const int r = r0 + lane;
+        if (r < a.mpad) a.p1[(size_t)j * a.mpad + r] = tile[jb][lane];
+    }
+}
+
+// ------------------------------------------------------------------------------------------ K2f
+struct FPass2Args {
+    const float2 *p1;
+    const double *tan_s, *kr_grid, *kc_grid, *ham_m, *ham_n;
+    const float *tabf;
+    const float2 *tw;
+    float2 *y1;
+    int m, n, mpad, centred, window;
+};
+
+template <int L, int E, bool SINC>
+__global__ void __launch_bounds__((1 << L) / E) k_fl_pass2_fft(FPass2Args a) {
+    using F = F32Fft<L, E>;
+    constexpr int N = F::N, T = F::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int m = a.m;
+    const size_t regA = max((size_t)8 * m, (size_t)8 * F::xbuf_elems());
+    float2 *row = reinterpret_cast<float2 *>(smem);
+    float2 *xbuf = reinterpret_cast<float2 *>(smem);
+    float *tab = reinterpret_cast<float *>(smem + regA);
+    const int tid = threadIdx.x;
+    const int j = blockIdx.x;
+    for (int r = tid; r < m; r += T) row[r] = a.p1[(size_t)j * a.mpad + r];
+    if (SINC)
+        for (int i = tid; i < 256 * 32; i += T) tab[i] = a.tabf[i];
+    __syncthreads();
+    const double krj = a.kr_grid[j];
+    const double s0 = krj * a.tan_s[0], s1 = krj * a.tan_s[m - 1];
+    const bool asc = s1 >= s0;
+    auto xa = [&](int t) { return krj * __ldg(a.tan_s + (asc ? t : m - 1 - t)); };
+    const double lo_v = asc ? s0 : s1, hi_v = asc ? s1 : s0;
+    const double inv_span = (double)(m - 1) / (hi_v - lo_v);
+    const double hn = a.window ? a.ham_n[j] : 1.0;
+    float2 x[E];
+#pragma unroll
+    for (int u = 0; u < E; ++u) {
+        const int k = tid + T * u;
+        float2 val = make_float2(0.f, 0.f);
+        if (k < m) {
+            const double q = a.kc_grid[k];
+            Frac fr{0.f, 0, 0};
+            const int g = isfinite(inv_span) ? (int)((q - lo_v) * inv_span) : 0;
+            const int ja = interp_bracket(xa, m, lo_v, hi_v, q, g, fr);
+            if (ja >= 0) {
+                int lowi = ja;
+                if (!asc) { lowi = m - 2 - ja; mirror_frac(fr); }
+                val = gather_f32<SINC>(row, 0, m, lowi, fr, tab);
+                // np.outer(hamming(m), hamming(n)).astype(float32)[k, j]
+                const float wgt = a.window ? (float)(a.ham_m[k] * hn) : 1.0f;
+                const float sg = (a.centred && ((j + k) & 1)) ? -wgt : wgt;
+                val.x *= sg;
+                val.y *= sg;
+            }
+        }
+        x[(int)(__brev((unsigned)u) >> (32 - F::LE))] = val;
+    }
+    F::run(x, xbuf, a.tw, tid);
+    float2 *out = a.y1 + (size_t)j * N;
+#pragma unroll
+    for (int v = 0; v < E; ++v) out[tid + T * v] = x[v];
+}
+
+// ------------------------------------------------------------------------------------------ K3f
+struct FFft2Args {
+    const float2 *y1;
+    const float2 *tw;
+    void *out;
+    int n, m2, centred, detect;
+    float scale;
+};
+
+template <int L, int E>
+__global__ void __launch_bounds__((1 << L) / E) k_fl_fft2(FFft2Args a) {
+    using F = F32Fft<L, E>;
+    constexpr int N = F::N, T = F::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2 *xbuf = reinterpret_cast<float2 *>(smem);
+    const int tid = threadIdx.x;
+    const int k = blockIdx.x;                  // cross bin (row of the output image)
+    float2 x[E];
+#pragma unroll
+    for (int u = 0; u < E; ++u) {
+        const int j = tid + T * u;
+        x[(int)(__brev((unsigned)u) >> (32 - F::LE))] =
+            j < a.n ? __ldg(a.y1 + (size_t)j * a.m2 + k) : make_float2(0.f, 0.f);
+    }
+    F::run(x, xbuf, a.tw, tid);
+    const size_t base = (size_t)k * N;
+#pragma unroll
+    for (int v = 0; v < E; ++v) {
+        const int col = tid + T * v;
+        float2 z = make_float2(x[v].x * a.scale, x[v].y * a.scale);
+        if (a.detect == PFA_DETECT_MAG) {
+            static_cast<float *>(a.out)[base + col] = sqrtf(fmaf(z.x, z.x, z.y * z.y));
+        } else if (a.detect == PFA_DETECT_POWER) {
+            static_cast<float *>(a.out)[base + col] = fmaf(z.x, z.x, z.y * z.y);
+        } else {
+            if (a.centred && ((k + col) & 1)) { z.x = -z.x; z.y = -z.y; }
+            static_cast<float2 *>(a.out)[base + col] = z;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------ launch
+template <int L>
+struct Cfg {
+    static constexpr int N = 1 << L;
+    static constexpr int E = (N >= 512) ? 16 : (N / 32);
+    static constexpr int T = N / E;
+};
+
+template <int L, bool SINC>
+cudaError_t launch_pass2(const FloatDev &d, cudaStream_t st) {
+    using F = F32Fft<L, Cfg<L>::E>;
+    FPass2Args p{d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabf,
+                 d.twm, d.y1, d.m, d.n, d.mpad, d.layout == PFA_LAYOUT_CENTRED, d.window};
+    size_t regA = std::max((size_t)8 * d.m, (size_t)8 * F::xbuf_elems());
+    size_t sm = regA + (SINC ? 256 * 32 * 4 : 0);
+    auto fn = k_fl_pass2_fft<L, Cfg<L>::E, SINC>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    fn<<<d.n, Cfg<L>::T, sm, st>>>(p);
+    return cudaGetLastError();
+}
+
+template <int L>
+cudaError_t launch_fft2(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st) {
+    using F = F32Fft<L, Cfg<L>::E>;
+    FFft2Args p{d.y1, d.twn, out, d.n, d.m2, d.layout == PFA_LAYOUT_CENTRED, detect, scale};
+    size_t sm = (size_t)8 * F::xbuf_elems();
+    auto fn = k_fl_fft2<L, Cfg<L>::E>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    fn<<<d.m2, Cfg<L>::T, sm, st>>>(p);
+    return cudaGetLastError();
+}
+
+template <bool SINC>
+cudaError_t dispatch_pass2(const FloatDev &d, cudaStream_t st) {
+    switch (d.Lm) {
+        case 6: return launch_pass2<6, SINC>(d, st);
+        case 7: return launch_pass2<7, SINC>(d, st);
+        case 8: return launch_pass2<8, SINC>(d, st);
+        case 9: return launch_pass2<9, SINC>(d, st);
+        case 10: return launch_pass2<10, SINC>(d, st);
+        case 11: return launch_pass2<11, SINC>(d, st);
+        case 12: return launch_pass2<12, SINC>(d, st);
+        case 13: return launch_pass2<13, SINC>(d, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t dispatch_fft2(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st) {
+    switch (d.Ln) {
+        case 6: return launch_fft2<6>(d, out, detect, scale, st);
+        case 7: return launch_fft2<7>(d, out, detect, scale, st);
+        case 8: return launch_fft2<8>(d, out, detect, scale, st);
+        case 9: return launch_fft2<9>(d, out, detect, scale, st);
+        case 10: return launch_fft2<10>(d, out, detect, scale, st);
+        case 11: return launch_fft2<11>(d, out, detect, scale, st);
+        case 12: return launch_fft2<12>(d, out, detect, scale, st);
+        case 13: return launch_fft2<13>(d, out, detect, scale, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+int ilog2i(int v) { int l = 0; while ((1 << l) < v) ++l; return l; }
+
+template <class T>
+cudaError_t dal(T **p, size_t cnt) { return cudaMalloc(reinterpret_cast<void **>(p), std::max<size_t>(cnt, 1) * sizeof(T)); }
+template <class T>
+void dfr(T *&p) { if (p) cudaFree(p); p = nullptr; }
+
+void stage_twiddles(int N, int sgn, std::vector<float2> &out) {
+    out.assign(std::max(N - 1, 1), make_float2(0.f, 0.f));
+    const int L = ilog2i(N);
+    for (int b = 0; b < L; ++b) {
+        const int span = 2 << b;
+        for (int k = 0; k < (1 << b); ++k) {
+            const double th = (sgn < 0 ? -2.0 : 2.0) * M_PI * (double)k / (double)span;
+            out[(1 << b) - 1 + k] = make_float2((float)std::cos(th), (float)std::sin(th));
+        }
+    }
+}
+
+}  // namespace
+
+size_t float_workspace_bytes(int m, int n) {
+    const int m2 = 1 << ilog2i(m), mpad = (m + 31) / 32 * 32;
+    return (size_t)8 * n * mpad + (size_t)8 * n * m2;
+}
+
+cudaError_t float_alloc(FloatDev &d, int m, int n) {
+    d.m = m; d.n = n;
+    d.Lm = ilog2i(m); d.Ln = ilog2i(n);
+    d.m2 = 1 << d.Lm; d.n2 = 1 << d.Ln;
+    d.mpad = (m + 31) / 32 * 32;
+    if (d.m2 < 64 || d.n2 < 64 || d.m2 > 8192 || d.n2 > 8192) return cudaErrorInvalidValue;
+    cudaError_t e;
+#define TRY(x) do { e = (x); if (e != cudaSuccess) return e; } while (0)
+    TRY(dal(&d.f0, m)); TRY(dal(&d.df, m)); TRY(dal(&d.flast, m)); TRY(dal(&d.pr, m)); TRY(dal(&d.tan_s, m)); TRY(dal(&d.order, m));
+    TRY(dal(&d.kr, n)); TRY(dal(&d.kc, m)); TRY(dal(&d.ham_m64, m)); TRY(dal(&d.ham_n64, n));
+    TRY(dal(&d.twm, d.m2)); TRY(dal(&d.twn, d.n2));
+    TRY(dal(&d.tabf, 256 * 32));
+    TRY(dal(&d.p1, (size_t)n * d.mpad)); TRY(dal(&d.y1, (size_t)n * d.m2));
+#undef TRY
+    return cudaSuccess;
+}
+
+void float_free(FloatDev &d) {
+    dfr(d.f0); dfr(d.df); dfr(d.flast); dfr(d.pr); dfr(d.tan_s); dfr(d.order); dfr(d.kr); dfr(d.kc); dfr(d.ham_m64);
+    dfr(d.ham_n64); dfr(d.twm); dfr(d.twn); dfr(d.tabf); dfr(d.p1); dfr(d.y1);
+}
+
+cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int detect, cudaStream_t st, StageProf *prof) {
+    StageProf none;
+    StageProf &pf = prof ? *prof : none;
+    pf.count = 0;
+    cudaError_t e = pf.mark(st, "start");
+    if (e != cudaSuccess) return e;
+    FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabf, d.p1, d.m, d.n, d.mpad};
+    dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + F1_BINS - 1) / F1_BINS);
+    if (d.range_sinc) {
+        e = cudaFuncSetAttribute(k_fl_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1_smem(true));
+        if (e != cudaSuccess) return e;
+        k_fl_pass1<true><<<g1, 256, f1_smem(true), st>>>(p1);
+    } else {
+        e = cudaFuncSetAttribute(k_fl_pass1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1_smem(false));
+        if (e != cudaSuccess) return e;
+        k_fl_pass1<false><<<g1, 256, f1_smem(false), st>>>(p1);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = pf.mark(st, "pass1")) != cudaSuccess) return e;
+    e = d.az_sinc ? dispatch_pass2<true>(d, st) : dispatch_pass2<false>(d, st);
+    if (e != cudaSuccess) return e;
+    if ((e = pf.mark(st, "pass2_win_fft1")) != cudaSuccess) return e;
+    const float scale = d.sgn > 0 ? 1.0f / ((float)d.m2 * (float)d.n2) : 1.0f;
+    e = dispatch_fft2(d, out, detect, scale, st);
+    if (e != cudaSuccess) return e;
+    return pf.mark(st, "fft2_detect");
+}
+
 }  // namespace pfa
 
-extern "C" {
-pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *) { return p ? PFA_ERR_BAD_CONFIG : PFA_ERR_BAD_ARG; }
-pfa_status pfa_form_float(pfa_plan *p, const float *, void *, int32_t, void *) { return p ? PFA_ERR_BAD_CONFIG : PFA_ERR_BAD_ARG; }
-pfa_status pfa_form_float_host(pfa_plan *p, const float *, void *, int32_t) { return p ? PFA_ERR_BAD_CONFIG : PFA_ERR_BAD_ARG; }
+// ------------------------------------------------------------------------------------------ C ABI
+namespace {
+pfa_status ffail(pfa_plan *p, pfa_status st, const char *msg) {
+    if (p) p->err = msg;
+    return st;
 }
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int dev) { if (cudaGetDevice(&prev) != cudaSuccess) prev = -1; if (prev != dev) cudaSetDevice(dev); }
+    ~DevGuard() { int cur = -1; if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev); }
+};
+pfa_status fcuda(pfa_plan *p, cudaError_t e, const char *where) {
+    if (p) p->err = std::string(where) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? PFA_ERR_ALLOC : PFA_ERR_CUDA;
+}
+}  // namespace
+
+extern "C" {
+
+pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *job) {
+    if (!p || !job) return PFA_ERR_BAD_ARG;
+    if (p->cfg.mode != PFA_MODE_FLOAT32 && p->cfg.mode != PFA_MODE_MIXED) return ffail(p, PFA_ERR_BAD_CONFIG, "plan is not float mode");
+    if (!job->f0 || !job->df || !job->f_last || !job->pr || !job->tan_s || !job->order || !job->kr_grid || !job->kc_grid)
+        return ffail(p, PFA_ERR_BAD_ARG, "missing job vector");
+    if (job->layout != PFA_LAYOUT_CENTRED && job->layout != PFA_LAYOUT_NATURAL) return ffail(p, PFA_ERR_BAD_ARG, "bad layout");
+    DevGuard dg(p->device);
+    pfa::FloatDev &d = p->fl;
+    const int m = d.m, n = d.n;
+    std::vector<int> seen(m, 0);
+    for (int i = 0; i < m; ++i) {
+        const int r = job->order[i];
+        if (r < 0 || r >= m || seen[r]++) return ffail(p, PFA_ERR_BAD_ARG, "order is not a permutation");
+    }
+    d.sgn = job->sgn < 0 ? -1 : 1;
+    d.layout = job->layout;
+    d.window = (job->ham_m && job->ham_n) ? 1 : 0;
+    std::vector<float2> twm, twn;
+    pfa::stage_twiddles(d.m2, d.sgn, twm);
+    pfa::stage_twiddles(d.n2, d.sgn, twn);
+    std::vector<float> tabf(256 * 32);
+    const int16_t *tq = pfa::builtin_sinc_table();
+    for (int i = 0; i < 256 * 32; ++i) tabf[i] = (float)tq[i] / 32768.0f;
+    cudaError_t e;
+#define CPY(dst, src, cnt) do { e = cudaMemcpy(dst, src, sizeof(*(dst)) * (cnt), cudaMemcpyHostToDevice); \
+        if (e != cudaSuccess) return fcuda(p, e, "float job upload"); } while (0)
+    CPY(d.f0, job->f0, m); CPY(d.df, job->df, m); CPY(d.flast, job->f_last, m); CPY(d.pr, job->pr, m); CPY(d.tan_s, job->tan_s, m);
+    CPY(d.order, job->order, m); CPY(d.kr, job->kr_grid, n); CPY(d.kc, job->kc_grid, m);
+    if (d.window) { CPY(d.ham_m64, job->ham_m, m); CPY(d.ham_n64, job->ham_n, n); }
+    CPY(d.twm, twm.data(), d.m2 - 1); CPY(d.twn, twn.data(), d.n2 - 1);
+    CPY(d.tabf, tabf.data(), 256 * 32);
+#undef CPY
+    p->job_ready = true;
+    return PFA_OK;
+}
+
+pfa_status pfa_form_float(pfa_plan *p, const float *sig_dev, void *out_dev, int32_t detect, void *stream) {
+    if (!p || !sig_dev || !out_dev) return PFA_ERR_BAD_ARG;
+    if (p->cfg.mode != PFA_MODE_FLOAT32 && p->cfg.mode != PFA_MODE_MIXED) return ffail(p, PFA_ERR_BAD_CONFIG, "plan is not float mode");
+    if (!p->job_ready) return ffail(p, PFA_ERR_NOT_READY, "pfa_set_float_job not called");
+    if (detect < PFA_DETECT_MAG || detect > PFA_DETECT_COMPLEX) return ffail(p, PFA_ERR_BAD_ARG, "bad detect mode");
+    if (reinterpret_cast<uintptr_t>(sig_dev) & 7) return ffail(p, PFA_ERR_BAD_ARG, "signal must be 8-byte aligned");
+    DevGuard dg(p->device);
+    cudaError_t e = pfa::float_form(p->fl, reinterpret_cast<const float2 *>(sig_dev), out_dev, detect,
+                                    reinterpret_cast<cudaStream_t>(stream), &p->prof);
+    if (e != cudaSuccess) return fcuda(p, e, "float form");
+    return PFA_OK;
+}
+
+pfa_status pfa_form_float_host(pfa_plan *p, const float *sig_host, void *out_host, int32_t detect) {
+    if (!p || !sig_host || !out_host) return PFA_ERR_BAD_ARG;
+    if (p->cfg.mode != PFA_MODE_FLOAT32 && p->cfg.mode != PFA_MODE_MIXED) return ffail(p, PFA_ERR_BAD_CONFIG, "plan is not float mode");
+    DevGuard dg(p->device);
+    const size_t in_b = sizeof(float) * 2 * (size_t)p->fl.m * p->fl.n;
+    const size_t out_b = (detect == PFA_DETECT_COMPLEX ? 8 : 4) * (size_t)p->fl.m2 * p->fl.n2;
+    cudaError_t e;
+    if (!p->host_stream && (e = cudaStreamCreateWithFlags(&p->host_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fcuda(p, e, "stream");
+    if (p->staging_in_bytes < in_b) {
+        if (p->staging_in) cudaFree(p->staging_in);
+        p->staging_in = nullptr;
+        if ((e = cudaMalloc(reinterpret_cast<void **>(&p->staging_in), in_b)) != cudaSuccess) { p->staging_in_bytes = 0; return fcuda(p, e, "staging"); }
+        p->staging_in_bytes = in_b;
+    }
+    if (p->staging_out_bytes < out_b) {
+        if (p->staging_out) cudaFree(p->staging_out);
+        p->staging_out = nullptr;
+        if ((e = cudaMalloc(&p->staging_out, out_b)) != cudaSuccess) { p->staging_out_bytes = 0; return fcuda(p, e, "staging"); }
+        p->staging_out_bytes = out_b;
+    }
+    if ((e = cudaMemcpyAsync(p->staging_in, sig_host, in_b, cudaMemcpyHostToDevice, p->host_stream)) != cudaSuccess)
+        return fcuda(p, e, "h2d");
+    pfa_status st = pfa_form_float(p, p->staging_in, p->staging_out, detect, p->host_stream);
+    if (st != PFA_OK) return st;
+    if ((e = cudaMemcpyAsync(out_host, p->staging_out, out_b, cudaMemcpyDeviceToHost, p->host_stream)) != cudaSuccess)
+        return fcuda(p, e, "d2h");
+    if ((e = cudaStreamSynchronize(p->host_stream)) != cudaSuccess) return fcuda(p, e, "sync");
+    return PFA_OK;
+}
+
+}  // extern "C"

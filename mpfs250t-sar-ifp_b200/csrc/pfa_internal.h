@@ -34,12 +34,12 @@ struct FixedDev {
 struct FloatDev {
     int m = 0, n = 0, m2 = 0, n2 = 0, Lm = 0, Ln = 0, mpad = 0;
     int range_sinc = 0, az_sinc = 0, sgn = -1, layout = 0;
-    double *f0 = nullptr, *df = nullptr, *pr = nullptr, *tan_s = nullptr, *kr = nullptr, *kc = nullptr;
+    double *f0 = nullptr, *df = nullptr, *flast = nullptr, *pr = nullptr, *tan_s = nullptr, *kr = nullptr, *kc = nullptr;
     float *ham_m = nullptr, *ham_n = nullptr;   // unused when window is off
     double *ham_m64 = nullptr, *ham_n64 = nullptr;
     int32_t *order = nullptr;
     float2 *twm = nullptr, *twn = nullptr;      // stage-contiguous twiddles for m2 and n2
-    int16_t *sinc = nullptr;
+    float *tabf = nullptr;                      // 256 x 32 sinc table / 32768
     int window = 1;
     float2 *p1 = nullptr;              // [n][mpad] pass-1 output (range-bin rows, sorted pulses)
     float2 *y1 = nullptr;              // [n][m2] cross FFT output (range-bin rows)

@@ -42,8 +42,8 @@ class FixedJob(C.Structure):
 
 
 class FloatJob(C.Structure):
-    _fields_ = [("f0", C.c_void_p), ("df", C.c_void_p), ("pr", C.c_void_p), ("tan_s", C.c_void_p),
-                ("order", C.c_void_p), ("kr_grid", C.c_void_p), ("kc_grid", C.c_void_p),
+    _fields_ = [("f0", C.c_void_p), ("df", C.c_void_p), ("f_last", C.c_void_p), ("pr", C.c_void_p),
+                ("tan_s", C.c_void_p), ("order", C.c_void_p), ("kr_grid", C.c_void_p), ("kc_grid", C.c_void_p),
                 ("ham_m", C.c_void_p), ("ham_n", C.c_void_p), ("sgn", C.c_int32), ("layout", C.c_int32)]
 
 

@@ -149,6 +149,65 @@ class FixedPlan(_Plan):
         return er, ea, int(q0.value)
 
 
+class FloatPlan(_Plan):
+    """Float PFA frame former: form_image_pfa.pfa + detection for an (m, n) scene onto the
+    (pow2(m), pow2(n)) raster, rows = cross, cols = range, centred as the reference (or natural)."""
+
+    DETECT = {"mag": _lib.DETECT_MAG, "power": _lib.DETECT_POWER, "complex": _lib.DETECT_COMPLEX}
+
+    def __init__(self, m: int, n: int, range_sinc: bool = False, az_sinc: bool = False, mixed: bool = False,
+                 device: int = 0):
+        cfg = _lib.Config(mode=_lib.MODE_MIXED if mixed else _lib.MODE_FLOAT32, m=m, n=n, grid=0,
+                          range_interp=_lib.SINC if range_sinc else _lib.LERP,
+                          az_interp=_lib.SINC if az_sinc else _lib.LERP, device=device)
+        super().__init__(cfg)
+        self.m, self.n, self.device = m, n, device
+        self.m2, self.n2 = geometry.pow2(m), geometry.pow2(n)
+
+    def set_tables(self, tables: dict, window: bool = True, centred: bool = True):
+        """Upload the job derived from ``prepare_tables`` output (mpfs/host/sar_pipeline.py:36-115)."""
+        job = geometry.float_job(tables)
+        keep = dict(f0=job["f0"], df=job["df"], fl=job["f_last"], pr=job["pr"], tan_s=job["tan_s"],
+                    order=job["order"], kr=job["KR"], kc=job["KC"], hm=np.ascontiguousarray(job["ham_m"]),
+                    hn=np.ascontiguousarray(job["ham_n"]))
+        fj = _lib.FloatJob(_ptr(keep["f0"]), _ptr(keep["df"]), _ptr(keep["fl"]), _ptr(keep["pr"]), _ptr(keep["tan_s"]),
+                           _ptr(keep["order"]), _ptr(keep["kr"]), _ptr(keep["kc"]),
+                           _ptr(keep["hm"]) if window else None, _ptr(keep["hn"]) if window else None,
+                           int(job["sgn"]), _lib.LAYOUT_CENTRED if centred else _lib.LAYOUT_NATURAL)
+        _lib.check(self._lib.pfa_set_float_job(self._h, C.byref(fj)), self._h)
+        self._job = keep
+
+    def form(self, signal, out=None, detect: str = "mag", stream=None):
+        """signal: (m, n) complex64 CUDA tensor (or NumPy array).  Returns (m2, n2) float32 |img|
+        (``detect="power"``: |img|^2, ``"complex"``: complex64 img)."""
+        torch = _torch()
+        host = isinstance(signal, np.ndarray)
+        sig = torch.from_numpy(np.ascontiguousarray(signal, np.complex64)).to(f"cuda:{self.device}") if host \
+            else signal.contiguous()
+        if sig.dtype != torch.complex64 or tuple(sig.shape) != (self.m, self.n):
+            raise ValueError(f"signal must be complex64 {(self.m, self.n)}, got {sig.dtype} {tuple(sig.shape)}")
+        dt = torch.complex64 if detect == "complex" else torch.float32
+        img = out if out is not None else torch.empty((self.m2, self.n2), dtype=dt, device=sig.device)
+        _lib.check(self._lib.pfa_form_float(self._h, C.c_void_p(sig.data_ptr()), C.c_void_p(img.data_ptr()),
+                                            self.DETECT[detect], _stream_handle(stream)), self._h)
+        return img.cpu().numpy() if host else img
+
+    def form_host(self, signal: np.ndarray, out: np.ndarray | None = None, detect: str = "mag") -> np.ndarray:
+        sig = np.ascontiguousarray(signal, np.complex64)
+        dt = np.complex64 if detect == "complex" else np.float32
+        img = out if out is not None else np.empty((self.m2, self.n2), dt)
+        _lib.check(self._lib.pfa_form_float_host(self._h, _ptr(sig), _ptr(img), self.DETECT[detect]), self._h)
+        return img
+
+
+def focus_float(signal, tables, range_sinc=False, az_sinc=False, mixed=False, device=0):
+    """Drop-in for ``accel.NumpyBackend.focus`` (mpfs/host/accel.py:39-44): float32 |img|."""
+    m, n = np.asarray(signal).shape if isinstance(signal, np.ndarray) else tuple(signal.shape)
+    with FloatPlan(m, n, range_sinc, az_sinc, mixed, device) as plan:
+        plan.set_tables(tables)
+        return plan.form(signal)
+
+
 def form_image_fixed(signal, tables, grid, range_sinc=False, az_sinc=False, device=0):
     """Drop-in for the emulator datapath: ``img = form_image_fixed(signal, tables, grid, rs, az)``
     replaces silicon_emulator.py:226-249 (Q0 quantise .. detect_fixed) and returns the same uint16

@@ -158,7 +158,8 @@ def float_job(tables: dict) -> dict:
     kc_max = max(abs(KR[0]), abs(KR[-1])) * np.abs(tan_phi).max()
     KC = np.asarray(tables.get("KC", np.linspace(-kc_max, kc_max, m)), np.float64)
     order = np.argsort(tan_phi)
-    return dict(m=m, n=n, m2=pow2(m), n2=pow2(n), f0=f0, df=df, pr=np.ascontiguousarray(pr),
+    f_last = np.ascontiguousarray(freq[:, -1], np.float64)
+    return dict(m=m, n=n, m2=pow2(m), n2=pow2(n), f0=f0, df=df, f_last=f_last, pr=np.ascontiguousarray(pr),
                 tan_s=np.ascontiguousarray(tan_phi[order]), order=order.astype(np.int32),
                 KR=np.ascontiguousarray(KR), KC=np.ascontiguousarray(KC),
                 ham_m=np.hamming(m), ham_n=np.hamming(n), sgn=int(tables.get("sgn", -1)))

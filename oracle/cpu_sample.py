@@ -131,3 +131,82 @@ def available_cores() -> int:
         return len(os.sched_getaffinity(0))
     except AttributeError:
         return os.cpu_count() or 1
+
+
+def _float_p1_chunk(args):
+    rows, kr, KR = args                      # rows: sampled pulses (complex64), kr: their wavenumbers
+    from . import float_pfa as fp
+    t = time.perf_counter()
+    for r in range(rows.shape[0]):
+        xp, row = kr[r], rows[r]
+        if xp[0] > xp[-1]:
+            xp, row = xp[::-1], row[::-1]
+        fp._interp(KR, xp, row, "lerp").astype(np.complex64)
+    return time.perf_counter() - t
+
+
+def _float_p2_chunk(args):
+    cols, KRs, tan_s, KC = args              # cols: (S, m) sorted-pulse columns of g1
+    from . import float_pfa as fp
+    t = time.perf_counter()
+    for c in range(cols.shape[0]):
+        fp._interp(KC, KRs[c] * tan_s, cols[c], "lerp").astype(np.complex64)
+    return time.perf_counter() - t
+
+
+def _float_fft_chunk(args):
+    x = args
+    t = time.perf_counter()
+    np.fft.fft(x, axis=-1)
+    return time.perf_counter() - t
+
+
+def float_frame_estimate(signal, tables, sample=64, workers=1, pool=None, seed=0):
+    """Estimated time (ms) of the reference-precision float PFA (form_image_pfa.resample_kspace + focus
+    + |.|, restated in oracle/float_pfa.py) for one frame, from `sample` lines per stage."""
+    from . import float_pfa as fp
+    rng = np.random.default_rng(seed)
+    g = fp.geometry(tables["freq"], tables["ax"], tables["ay"])
+    m, n = g["m"], g["n"]
+    m2, n2 = fp.to_pow2(m), fp.to_pow2(n)
+    s1, s2 = min(sample, m), min(sample, n)
+    p1_rows = np.linspace(0, m - 1, s1).astype(int)
+    p2_rows = np.linspace(0, n - 1, s2).astype(int)
+    cols = (rng.standard_normal((s2, m)) + 1j * rng.standard_normal((s2, m))).astype(np.complex64)
+    tan_s = g["tan_phi"][g["order"]]
+    fr = (rng.standard_normal((min(sample, m2), n2)) + 1j * rng.standard_normal((min(sample, m2), n2))).astype(np.complex64)
+    fc = (rng.standard_normal((min(sample, n2), m2)) + 1j * rng.standard_normal((min(sample, n2), m2))).astype(np.complex64)
+
+    def split(rows):
+        return [c for c in np.array_split(rows, workers) if len(c)]
+
+    own = False
+    if workers > 1:
+        ex = pool
+        if ex is None:
+            ex, own = make_pool(workers), True
+        run = lambda fn, jobs: max(ex.map(fn, jobs)) if jobs else 0.0   # noqa: E731
+    else:
+        ex = None
+        run = lambda fn, jobs: sum(map(fn, jobs))                          # noqa: E731
+    stage = {}
+    try:
+        if ex is not None:
+            list(ex.map(_float_fft_chunk, [fr[:1, :64]] * workers))
+        stage["pass1"] = run(_float_p1_chunk, [(np.asarray(signal)[c], g["kr"][c], g["KR"]) for c in split(p1_rows)]) * m / s1
+        stage["pass2"] = run(_float_p2_chunk, [(cols[c], g["KR"][p2_rows[c]], tan_s, g["KC"]) for c in split(np.arange(s2))]) * n / s2
+        t = time.perf_counter()
+        _ = np.asarray(signal[:s1]) * np.float32(1.0)                 # window multiply, sampled
+        stage["window"] = (time.perf_counter() - t) * m / s1
+        stage["fft_rows"] = run(_float_fft_chunk, [fr[c] for c in split(np.arange(fr.shape[0]))]) * m2 / fr.shape[0]
+        stage["fft_cols"] = run(_float_fft_chunk, [fc[c] for c in split(np.arange(fc.shape[0]))]) * n2 / fc.shape[0]
+        t = time.perf_counter()
+        np.abs(fr).astype(np.float32)
+        stage["detect"] = (time.perf_counter() - t) * m2 / fr.shape[0]
+    finally:
+        if own:
+            ex.shutdown()
+    total = sum(stage.values())
+    return dict(ms_per_frame=1000.0 * total, stage_seconds={k: round(v, 4) for k, v in stage.items()},
+                sample=f"{s1} of {m} pulses, {s2} of {n} range bins, {fr.shape[0]} of {m2} FFT rows and "
+                       f"{fc.shape[0]} of {n2} FFT columns, scaled to the full frame", workers=workers)
