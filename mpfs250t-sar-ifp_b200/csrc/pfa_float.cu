@@ -11,6 +11,7 @@
 //
 // Centring: fftshift(fft(ifftshift(x)))[v] = (-1)^v fft((-1)^a x[a])[v] for even N with N/2 even, so the
 // shifts of form_image_pfa.transform2d (:144-147) cost one sign flip on load and one on store.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -18,6 +19,7 @@
 #include <cstring>
 #include <vector>
 
+#include "fft_f32.cuh"
 #include "pfa_internal.h"
 
 namespace pfa {
@@ -27,70 +29,17 @@ namespace {
 
 constexpr double kC = 299792458.0;
 
-// ------------------------------------------------------------------------------------------ FFT
-// Radix-2 DIT FFT in registers (E complex values per thread, T = N/E threads), bit groups of LE
-// stages between shared-memory exchanges -- the same thread/position mapping as the fixed-point
-// transform.  Twiddles: stage-contiguous table (stage b: 2^b entries at offset 2^b - 1).
+// FFT: register Stockham radix-16 (fft_f32.cuh).
 template <int L, int E>
-struct F32Fft {
-    static constexpr int N = 1 << L;
-    static constexpr int LE = (E == 16) ? 4 : (E == 8) ? 3 : (E == 4) ? 2 : 1;
-    static constexpr int T = N / E;
-    static constexpr int TB = L - LE;
-    static constexpr int NG = (L + LE - 1) / LE;
-    static_assert(T >= 32, "at least one warp");
+using F32Fft = StockhamFft<L, E>;
 
-    __device__ static __forceinline__ int group_lo(int g) { return (g * LE + LE <= L) ? g * LE : (L - LE); }
-    __device__ static __forceinline__ int pos(int lo, int t, int v) {
-        return (t & ((1 << lo) - 1)) | (v << lo) | ((t >> lo) << (lo + LE));
-    }
-    __device__ static __forceinline__ int swz(int p) { return p + (p >> 4); }
-    __device__ static __forceinline__ int logical(int g, int tid) {
-        return g == 0 ? (int)(__brev((unsigned)tid) >> (32 - TB)) : tid;
-    }
-    static constexpr int xbuf_elems() { return N + N / 16; }
-
-    // In: group-0 layout (element v of thread tid = natural index tid + T * bitrev(v)).
-    // Out: element v of thread tid = frequency index tid + T * v.
-    __device__ static void run(float2 (&x)[E], float2 *xbuf, const float2 *__restrict__ tw, int tid) {
-        int done = 0;
-#pragma unroll
-        for (int g = 0; g < NG; ++g) {
-            const int lo = group_lo(g);
-            const int t = logical(g, tid);
-            if (g > 0) {
-                const int plo = group_lo(g - 1);
-                const int pt = logical(g - 1, tid);
-                __syncthreads();
-#pragma unroll
-                for (int v = 0; v < E; ++v) xbuf[swz(pos(plo, pt, v))] = x[v];
-                __syncthreads();
-#pragma unroll
-                for (int v = 0; v < E; ++v) x[v] = xbuf[swz(pos(lo, t, v))];
-            }
-            const int tlow = t & ((1 << lo) - 1);
-#pragma unroll
-            for (int rb = 0; rb < LE; ++rb) {
-                const int b = lo + rb;
-                if (b < done) continue;
-                const float2 *tws = tw + ((1 << b) - 1);
-#pragma unroll
-                for (int v = 0; v < E; ++v) {
-                    if (v & (1 << rb)) continue;
-                    const int v2 = v | (1 << rb);
-                    const int k = tlow | ((v & ((1 << rb) - 1)) << lo);
-                    const float2 w = __ldg(tws + k);
-                    const float2 bb = x[v2];
-                    const float2 tt = make_float2(fmaf(w.x, bb.x, -w.y * bb.y), fmaf(w.x, bb.y, w.y * bb.x));
-                    const float2 a = x[v];
-                    x[v] = make_float2(a.x + tt.x, a.y + tt.y);
-                    x[v2] = make_float2(a.x - tt.x, a.y - tt.y);
-                }
-            }
-            done = lo + LE;
-        }
-    }
-};
+// ------------------------------------------------------------------------------------------ async copies
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // ------------------------------------------------------------------------------------------ brackets
 // np.interp bracket on an ascending accessor xa(0..n-1): returns j with xa(j) <= x < xa(j+1) and the
@@ -101,41 +50,60 @@ struct Frac {
     int rev;     // descending source axis: taps run in reverse natural order
 };
 
-template <class F>
+// phase of the float sinc from a float64 fraction (same rounding as the oracle's np.round)
+__device__ __forceinline__ int sinc_phase(double fd) {
+    return (int)fmin(fmax(rint(fd * 32768.0), 0.0), 32767.0) >> 7;
+}
+
+// Walks from the guess carrying both end values (two loads when the guess is right); bisection after a
+// few steps.  EXACT: float64 fraction (the sinc phase depends on it); else a float32 division.
+template <bool EXACT, class F>
 __device__ __forceinline__ int interp_bracket(const F &xa, int n, double x0, double x1, double x, int guess, Frac &frac) {
     if (!(x >= x0) || !(x <= x1)) return -1;
-    // largest j with xa(j) <= x
-    int j = min(max(guess, 0), n - 1);
+    // largest j in [0, n-2] with xa(j) <= x  (xa(0) = x0 <= x <= x1 = xa(n-1))
+    int j = min(max(guess, 0), n - 2);
+    double a = xa(j), b = xa(j + 1);
     int steps = 0;
-    while (j + 1 < n && xa(j + 1) <= x) {
+    while (b <= x && j < n - 2) {
+        if (++steps > 8) {
+            int lo = j + 1, hi = n - 2;      // xa(j+1) <= x
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (xa(mid) <= x) lo = mid; else hi = mid - 1;
+            }
+            j = lo;
+            a = xa(j);
+            b = xa(j + 1);
+            break;
+        }
         ++j;
-        if (++steps > 6) {
-            int lo = j, hi = n - 1;          // xa(lo) <= x; find the last index with xa <= x
+        a = b;
+        b = xa(j + 1);
+    }
+    while (a > x && j > 0) {
+        if (++steps > 16) {
+            int lo = 0, hi = j - 1;          // xa(0) <= x < xa(j)
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
                 if (xa(mid) <= x) lo = mid; else hi = mid - 1;
             }
             j = lo;
+            a = xa(j);
+            b = xa(j + 1);
             break;
         }
-    }
-    while (j > 0 && xa(j) > x) {
         --j;
-        if (++steps > 12) {
-            int lo = 0, hi = j;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (xa(mid) <= x) lo = mid; else hi = mid - 1;
-            }
-            j = lo;
-            break;
-        }
+        b = a;
+        a = xa(j);
     }
-    if (j >= n - 1) j = n - 2;
-    const double a = xa(j), b = xa(j + 1);
-    const double fd = __ddiv_rn(__dsub_rn(x, a), __dsub_rn(b, a));
-    frac.f = (float)fd;
-    frac.ph = (int)fmin(rint(__dmul_rn(fd, 32768.0)), 32767.0) >> 7;
+    if (EXACT) {
+        const double fd = __ddiv_rn(__dsub_rn(x, a), __dsub_rn(b, a));
+        frac.f = (float)fd;
+        frac.ph = sinc_phase(fd);
+    } else {
+        frac.f = __fdiv_rn((float)(x - a), (float)(b - a));
+        frac.ph = 0;
+    }
     frac.rev = 0;
     return j;
 }
@@ -215,7 +183,7 @@ __global__ void __launch_bounds__(256) k_fl_pass1(FPass1Args a) {
         const bool asc = kr(n - 1) >= kr(0);
         auto xa = [&](int t) { return asc ? kr(t) : kr(n - 1 - t); };
         const double xa0 = xa(0), xa1 = xa(n - 1);
-        const double inv = 1.0 / (sc * df);
+        const double inv_dk = 1.0 / fabs(sc * df);       // the source axis is affine in the sample index
         int jj[F1_BINS / 32];
         Frac fr[F1_BINS / 32];
         int lo_i = 1 << 30, hi_i = -1;
@@ -226,10 +194,15 @@ __global__ void __launch_bounds__(256) k_fl_pass1(FPass1Args a) {
             fr[t] = Frac{0.f, 0, 0};
             if (j < n) {
                 const double q = a.kr_grid[j];
-                const double kest = q * inv - f0 / df;
-                int g = 0;
-                if (isfinite(kest)) g = (int)fmin(fmax(asc ? floor(kest) : floor((double)(n - 1) - kest), 0.0), (double)(n - 1));
-                const int ja = interp_bracket(xa, n, xa0, xa1, q, g, fr[t]);
+                int ja = -1;
+                if (q >= xa0 && q <= xa1) {
+                    // closed-form bracket on the affine axis; the end points are exact
+                    const double pos = (q - xa0) * inv_dk;
+                    ja = isfinite(pos) ? min(max((int)floor(pos), 0), n - 2) : 0;
+                    const double fd = (q - xa(ja)) * inv_dk;
+                    fr[t].f = (float)fd;
+                    fr[t].ph = sinc_phase(fd);
+                }
                 if (ja >= 0) {
                     // natural-order index of the lower sample and the weight toward the upper one
                     int lowi;
@@ -278,26 +251,42 @@ struct FPass2Args {
     const double *tan_s, *kr_grid, *kc_grid, *ham_m, *ham_n;
     const float *tabf;
     const float2 *tw;
-    float2 *y1;
-    int m, n, mpad, centred, window;
+    float2 *y1t;          // [m2][npad] cross-FFT output, transposed: row = cross bin, col = range bin
+    int m, n, mpad, npad, centred, window, inverse;
 };
 
+// Corner turn #2 fused into the cross FFT: a cluster of kCT CTAs holds kCT adjacent range bins; after
+// their FFTs each CTA writes a 1/kCT slice of cross bins for all kCT rows (kCT * 8-byte runs) into the
+// transposed buffer, reading the other rows from the cluster's distributed shared memory.
+constexpr int kCT = 8;
+
 template <int L, int E, bool SINC>
-__global__ void __launch_bounds__((1 << L) / E) k_fl_pass2_fft(FPass2Args a) {
+__global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4)
+k_fl_pass2_fft(FPass2Args a) {
     using F = F32Fft<L, E>;
     constexpr int N = F::N, T = F::T;
     extern __shared__ __align__(16) unsigned char smem[];
     const int m = a.m;
-    const size_t regA = max((size_t)8 * m, (size_t)8 * F::xbuf_elems());
+    const size_t regA = (max((size_t)8 * m, (size_t)8 * F::xbuf_elems()) + 15) & ~(size_t)15;
     float2 *row = reinterpret_cast<float2 *>(smem);
     float2 *xbuf = reinterpret_cast<float2 *>(smem);
     float *tab = reinterpret_cast<float *>(smem + regA);
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
     const int tid = threadIdx.x;
     const int j = blockIdx.x;
-    for (int r = tid; r < m; r += T) row[r] = a.p1[(size_t)j * a.mpad + r];
-    if (SINC)
-        for (int i = tid; i < 256 * 32; i += T) tab[i] = a.tabf[i];
-    __syncthreads();
+    const bool live = j < a.n;                 // grid is padded to a multiple of the cluster size
+    float2 x[E];
+    if (live) {
+    // the row (and the sinc table) stream into shared memory while the brackets are computed
+    {
+        const float2 *src = a.p1 + (size_t)j * a.mpad;      // 256-byte aligned rows
+        const int nchunk = (m + 1) >> 1;                      // 16-byte chunks (the pad covers odd m)
+        for (int c = tid; c < nchunk; c += T) cp_async16(row + 2 * c, src + 2 * c);
+        if (SINC)
+            for (int c = tid; c < 256 * 32 / 4; c += T) cp_async16(tab + 4 * c, a.tabf + 4 * c);
+        cp_async_commit();
+    }
     const double krj = a.kr_grid[j];
     const double s0 = krj * a.tan_s[0], s1 = krj * a.tan_s[m - 1];
     const bool asc = s1 >= s0;
@@ -305,19 +294,36 @@ __global__ void __launch_bounds__((1 << L) / E) k_fl_pass2_fft(FPass2Args a) {
     const double lo_v = asc ? s0 : s1, hi_v = asc ? s1 : s0;
     const double inv_span = (double)(m - 1) / (hi_v - lo_v);
     const double hn = a.window ? a.ham_n[j] : 1.0;
-    float2 x[E];
+    int bl[E];      // packed bracket: lower natural index | phase << 16 | reversed << 24; -1 = outside
+    float bf[E];    // lerp weight toward the upper sample
+#pragma unroll
+    for (int u = 0; u < E; ++u) {
+        const int k = tid + T * u;
+        bl[u] = -1;
+        bf[u] = 0.f;
+        if (k < m) {
+            const double q = a.kc_grid[k];
+            Frac fr{0.f, 0, 0};
+            const int g = isfinite(inv_span) ? (int)((q - lo_v) * inv_span) : 0;
+            const int ja = interp_bracket<SINC>(xa, m, lo_v, hi_v, q, g, fr);
+            if (ja >= 0) {
+                int lowi = ja;
+                if (!asc) { lowi = m - 2 - ja; mirror_frac(fr); }
+                bl[u] = lowi | (fr.ph << 16) | (fr.rev << 24);
+                bf[u] = fr.f;
+            }
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
 #pragma unroll
     for (int u = 0; u < E; ++u) {
         const int k = tid + T * u;
         float2 val = make_float2(0.f, 0.f);
         if (k < m) {
-            const double q = a.kc_grid[k];
-            Frac fr{0.f, 0, 0};
-            const int g = isfinite(inv_span) ? (int)((q - lo_v) * inv_span) : 0;
-            const int ja = interp_bracket(xa, m, lo_v, hi_v, q, g, fr);
-            if (ja >= 0) {
-                int lowi = ja;
-                if (!asc) { lowi = m - 2 - ja; mirror_frac(fr); }
+            if (bl[u] >= 0) {
+                const int lowi = bl[u] & 0xffff;
+                const Frac fr{bf[u], (bl[u] >> 16) & 0xff, (bl[u] >> 24) & 1};
                 val = gather_f32<SINC>(row, 0, m, lowi, fr, tab);
                 // np.outer(hamming(m), hamming(n)).astype(float32)[k, j]
                 const float wgt = a.window ? (float)(a.ham_m[k] * hn) : 1.0f;
@@ -326,25 +332,43 @@ __global__ void __launch_bounds__((1 << L) / E) k_fl_pass2_fft(FPass2Args a) {
                 val.y *= sg;
             }
         }
-        x[(int)(__brev((unsigned)u) >> (32 - F::LE))] = val;
+        x[u] = a.inverse ? make_float2(val.x, -val.y) : val;
     }
     F::run(x, xbuf, a.tw, tid);
-    float2 *out = a.y1 + (size_t)j * N;
+    } else {
 #pragma unroll
-    for (int v = 0; v < E; ++v) out[tid + T * v] = x[v];
+        for (int v = 0; v < E; ++v) x[v] = make_float2(0.f, 0.f);
+    }
+    // exchange buffer: this CTA's FFT row in natural frequency order (stays conjugated for the inverse)
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < E; ++v) xbuf[tid + T * v] = x[v];
+    cluster.sync();
+    const int rank = (int)cluster.block_rank();
+    const int j0 = j - rank;
+    constexpr int SLICE = N / kCT;
+#pragma unroll
+    for (int s2 = 0; s2 < E; ++s2) {
+        const int item = tid + T * s2;         // item = kk * kCT + r
+        const int r = item % kCT;
+        const int k = rank * SLICE + item / kCT;
+        const float2 *remote = cluster.map_shared_rank(xbuf, r);
+        a.y1t[(size_t)k * a.npad + j0 + r] = remote[k];
+    }
+    cluster.sync();                            // keep this CTA's shared memory alive for the readers
 }
 
 // ------------------------------------------------------------------------------------------ K3f
 struct FFft2Args {
-    const float2 *y1;
+    const float2 *y1t;
     const float2 *tw;
     void *out;
-    int n, m2, centred, detect;
+    int n, npad, centred, detect, inverse;
     float scale;
 };
 
 template <int L, int E>
-__global__ void __launch_bounds__((1 << L) / E) k_fl_fft2(FFft2Args a) {
+__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4) k_fl_fft2(FFft2Args a) {
     using F = F32Fft<L, E>;
     constexpr int N = F::N, T = F::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -352,18 +376,19 @@ __global__ void __launch_bounds__((1 << L) / E) k_fl_fft2(FFft2Args a) {
     const int tid = threadIdx.x;
     const int k = blockIdx.x;                  // cross bin (row of the output image)
     float2 x[E];
+    const float2 *rowk = a.y1t + (size_t)k * a.npad;
 #pragma unroll
     for (int u = 0; u < E; ++u) {
         const int j = tid + T * u;
-        x[(int)(__brev((unsigned)u) >> (32 - F::LE))] =
-            j < a.n ? __ldg(a.y1 + (size_t)j * a.m2 + k) : make_float2(0.f, 0.f);
+        x[u] = j < a.n ? __ldcs(rowk + j) : make_float2(0.f, 0.f);
     }
     F::run(x, xbuf, a.tw, tid);
     const size_t base = (size_t)k * N;
+    const float cs = a.inverse ? -a.scale : a.scale;     // inverse: conj(FFT(conj(x))) / (m2 n2)
 #pragma unroll
     for (int v = 0; v < E; ++v) {
         const int col = tid + T * v;
-        float2 z = make_float2(x[v].x * a.scale, x[v].y * a.scale);
+        float2 z = make_float2(x[v].x * a.scale, x[v].y * cs);
         if (a.detect == PFA_DETECT_MAG) {
             static_cast<float *>(a.out)[base + col] = sqrtf(fmaf(z.x, z.x, z.y * z.y));
         } else if (a.detect == PFA_DETECT_POWER) {
@@ -387,20 +412,20 @@ template <int L, bool SINC>
 cudaError_t launch_pass2(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, Cfg<L>::E>;
     FPass2Args p{d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabf,
-                 d.twm, d.y1, d.m, d.n, d.mpad, d.layout == PFA_LAYOUT_CENTRED, d.window};
-    size_t regA = std::max((size_t)8 * d.m, (size_t)8 * F::xbuf_elems());
+                 d.twm, d.y1, d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0};
+    size_t regA = (std::max((size_t)8 * d.m, (size_t)8 * F::xbuf_elems()) + 15) & ~(size_t)15;
     size_t sm = regA + (SINC ? 256 * 32 * 4 : 0);
     auto fn = k_fl_pass2_fft<L, Cfg<L>::E, SINC>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    fn<<<d.n, Cfg<L>::T, sm, st>>>(p);
+    fn<<<d.npad, Cfg<L>::T, sm, st>>>(p);
     return cudaGetLastError();
 }
 
 template <int L>
 cudaError_t launch_fft2(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st) {
     using F = F32Fft<L, Cfg<L>::E>;
-    FFft2Args p{d.y1, d.twn, out, d.n, d.m2, d.layout == PFA_LAYOUT_CENTRED, detect, scale};
+    FFft2Args p{d.y1, d.twn, out, d.n, d.npad, d.layout == PFA_LAYOUT_CENTRED, detect, d.sgn > 0, scale};
     size_t sm = (size_t)8 * F::xbuf_elems();
     auto fn = k_fl_fft2<L, Cfg<L>::E>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -445,15 +470,12 @@ cudaError_t dal(T **p, size_t cnt) { return cudaMalloc(reinterpret_cast<void **>
 template <class T>
 void dfr(T *&p) { if (p) cudaFree(p); p = nullptr; }
 
-void stage_twiddles(int N, int sgn, std::vector<float2> &out) {
-    out.assign(std::max(N - 1, 1), make_float2(0.f, 0.f));
-    const int L = ilog2i(N);
-    for (int b = 0; b < L; ++b) {
-        const int span = 2 << b;
-        for (int k = 0; k < (1 << b); ++k) {
-            const double th = (sgn < 0 ? -2.0 : 2.0) * M_PI * (double)k / (double)span;
-            out[(1 << b) - 1 + k] = make_float2((float)std::cos(th), (float)std::sin(th));
-        }
+// W_N^k = exp(-2 pi i k / N), k < N (the inverse transform conjugates data, not twiddles)
+void full_twiddles(int N, std::vector<float2> &out) {
+    out.resize(N);
+    for (int k = 0; k < N; ++k) {
+        const double th = -2.0 * M_PI * (double)k / (double)N;
+        out[k] = make_float2((float)std::cos(th), (float)std::sin(th));
     }
 }
 
@@ -461,7 +483,8 @@ void stage_twiddles(int N, int sgn, std::vector<float2> &out) {
 
 size_t float_workspace_bytes(int m, int n) {
     const int m2 = 1 << ilog2i(m), mpad = (m + 31) / 32 * 32;
-    return (size_t)8 * n * mpad + (size_t)8 * n * m2;
+    const int npad = (n + 7) / 8 * 8;
+    return (size_t)8 * n * mpad + (size_t)8 * npad * m2;
 }
 
 cudaError_t float_alloc(FloatDev &d, int m, int n) {
@@ -469,6 +492,7 @@ cudaError_t float_alloc(FloatDev &d, int m, int n) {
     d.Lm = ilog2i(m); d.Ln = ilog2i(n);
     d.m2 = 1 << d.Lm; d.n2 = 1 << d.Ln;
     d.mpad = (m + 31) / 32 * 32;
+    d.npad = (n + kCT - 1) / kCT * kCT;
     if (d.m2 < 64 || d.n2 < 64 || d.m2 > 8192 || d.n2 > 8192) return cudaErrorInvalidValue;
     cudaError_t e;
 #define TRY(x) do { e = (x); if (e != cudaSuccess) return e; } while (0)
@@ -476,7 +500,7 @@ cudaError_t float_alloc(FloatDev &d, int m, int n) {
     TRY(dal(&d.kr, n)); TRY(dal(&d.kc, m)); TRY(dal(&d.ham_m64, m)); TRY(dal(&d.ham_n64, n));
     TRY(dal(&d.twm, d.m2)); TRY(dal(&d.twn, d.n2));
     TRY(dal(&d.tabf, 256 * 32));
-    TRY(dal(&d.p1, (size_t)n * d.mpad)); TRY(dal(&d.y1, (size_t)n * d.m2));
+    TRY(dal(&d.p1, (size_t)n * d.mpad)); TRY(dal(&d.y1, (size_t)d.npad * d.m2));
 #undef TRY
     return cudaSuccess;
 }
@@ -553,8 +577,8 @@ pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *job) {
     d.layout = job->layout;
     d.window = (job->ham_m && job->ham_n) ? 1 : 0;
     std::vector<float2> twm, twn;
-    pfa::stage_twiddles(d.m2, d.sgn, twm);
-    pfa::stage_twiddles(d.n2, d.sgn, twn);
+    pfa::full_twiddles(d.m2, twm);
+    pfa::full_twiddles(d.n2, twn);
     std::vector<float> tabf(256 * 32);
     const int16_t *tq = pfa::builtin_sinc_table();
     for (int i = 0; i < 256 * 32; ++i) tabf[i] = (float)tq[i] / 32768.0f;
@@ -564,7 +588,7 @@ pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *job) {
     CPY(d.f0, job->f0, m); CPY(d.df, job->df, m); CPY(d.flast, job->f_last, m); CPY(d.pr, job->pr, m); CPY(d.tan_s, job->tan_s, m);
     CPY(d.order, job->order, m); CPY(d.kr, job->kr_grid, n); CPY(d.kc, job->kc_grid, m);
     if (d.window) { CPY(d.ham_m64, job->ham_m, m); CPY(d.ham_n64, job->ham_n, n); }
-    CPY(d.twm, twm.data(), d.m2 - 1); CPY(d.twn, twn.data(), d.n2 - 1);
+    CPY(d.twm, twm.data(), d.m2); CPY(d.twn, twn.data(), d.n2);
     CPY(d.tabf, tabf.data(), 256 * 32);
 #undef CPY
     p->job_ready = true;

@@ -32,7 +32,7 @@ struct FixedDev {
 };
 
 struct FloatDev {
-    int m = 0, n = 0, m2 = 0, n2 = 0, Lm = 0, Ln = 0, mpad = 0;
+    int m = 0, n = 0, m2 = 0, n2 = 0, Lm = 0, Ln = 0, mpad = 0, npad = 0;
     int range_sinc = 0, az_sinc = 0, sgn = -1, layout = 0;
     double *f0 = nullptr, *df = nullptr, *flast = nullptr, *pr = nullptr, *tan_s = nullptr, *kr = nullptr, *kc = nullptr;
     float *ham_m = nullptr, *ham_n = nullptr;   // unused when window is off
@@ -42,7 +42,7 @@ struct FloatDev {
     float *tabf = nullptr;                      // 256 x 32 sinc table / 32768
     int window = 1;
     float2 *p1 = nullptr;              // [n][mpad] pass-1 output (range-bin rows, sorted pulses)
-    float2 *y1 = nullptr;              // [n][m2] cross FFT output (range-bin rows)
+    float2 *y1 = nullptr;              // [m2][npad] cross FFT output, transposed (cross-bin rows)
 };
 
 }  // namespace pfa
