@@ -162,6 +162,15 @@ pfa_status pfa_get_fixed_exponents(pfa_plan *plan, int32_t *e_range, int32_t *e_
 pfa_status pfa_form_float(pfa_plan *plan, const float *sig_dev, void *out_dev, int32_t detect, void *stream);
 pfa_status pfa_form_float_host(pfa_plan *plan, const float *sig_host, void *out_host, int32_t detect);
 
+/* Image-entropy autofocus.  For the per-pulse phase correction theta[m] (float32, device) the plan
+ * forms the float image of s[i,k] exp(-j theta_i) (lerp passes, window as set, natural layout), its
+ * entropy E = -sum p log p with p = |z|^2 / sum |z|^2, and dE/dtheta[m] with hand-written adjoint
+ * kernels (range FFT recomputed, adjoint FFTs, window, transposed pass-2 resample as an atomics-free
+ * segmented reduction).  entropy_dev (double, device) may be NULL.  The reference has no autofocus;
+ * the image it forms is form_image_pfa.pfa (src/form_image_pfa.py:243-246). */
+pfa_status pfa_autofocus_grad(pfa_plan *plan, const float *sig_dev, const float *theta_dev, float *dtheta_dev,
+                              double *entropy_dev, void *stream);
+
 /* Per-stage device timing, the counterpart of the board's per-stage timestamps sar_stage_ts[]
  * (sar_sequencer.c:235-238) and form_image_pfa.StepTimer (src/form_image_pfa.py:42-60).  When enabled,
  * every form call records CUDA events between its kernels on the launching stream.

@@ -144,6 +144,7 @@ struct FPass1Args {
     const double *f0, *df, *flast, *pr, *kr_grid;
     const int32_t *order;
     const float *tabf;
+    const float *theta;     // per-pulse phase correction exp(-j theta_i) (autofocus), or nullptr
     float2 *p1;
     int m, n, mpad;
 };
@@ -223,6 +224,13 @@ __global__ void __launch_bounds__(256) k_fl_pass1(FPass1Args a) {
         const bool fits = whi - wlo <= F1_WMAX;
         float2 *w = win[warp];
         const float2 *row = a.sig + (size_t)i * n;
+        // the phase correction commutes with the (linear, per-pulse) interpolation: rotate the output
+        float2 rot = make_float2(1.f, 0.f);
+        if (a.theta) {
+            float sn, cs;
+            sincosf(a.theta[i], &sn, &cs);
+            rot = make_float2(cs, -sn);
+        }
         if (fits)
             for (int k = wlo + lane; k < whi; k += 32) w[k - wlo] = row[k];
         __syncwarp();
@@ -232,7 +240,7 @@ __global__ void __launch_bounds__(256) k_fl_pass1(FPass1Args a) {
             float2 out = make_float2(0.f, 0.f);
             if (j0 + jb < n && jj[t] >= 0)
                 out = fits ? gather_f32<SINC>(w, wlo, n, jj[t], fr[t], tab) : gather_f32<SINC>(row, 0, n, jj[t], fr[t], tab);
-            tile[jb][slot] = out;
+            tile[jb][slot] = a.theta ? cmul(out, rot) : out;
         }
         __syncwarp();
     }
@@ -400,6 +408,208 @@ __global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4) k
     }
 }
 
+// ------------------------------------------------------------------------------------------ autofocus
+// Image-entropy autofocus gradient.  With x = s exp(-j theta) (applied in pass 1), p1 = R1 x,
+// z = F_range F_cross (W . R2 p1), I = |z|^2 and E = -sum p log p (p = I / S):
+//   g_z  = dE/dconj(z) = -(1/S)(log(I/S) + E) z                     (0 where I = 0)
+//   g_p1 = R2^H (W . F_cross^H F_range^H g_z)
+//   dE/dtheta_i = 2 Im sum_j conj(g_p1[j, slot_i]) p1[j, slot_i]     (pass 1 is linear and per pulse,
+//                 so its adjoint never has to be formed)
+// The range FFT is recomputed from the cross-FFT buffer in the adjoint pass instead of storing z.
+struct AfRangeArgs {
+    const float2 *y1t;      // [m2][npad] forward cross-FFT output, transposed
+    const float2 *tw;       // range twiddles (n2)
+    double *acc;            // [0] sum I, [1] sum I log I
+    float2 *zadj_t;         // [n][m2] F_range^H g_z, range-bin rows
+    int n, npad, m2;
+};
+
+template <int L, int E>
+__device__ __forceinline__ void af_load_range_row(float2 (&x)[E], const AfRangeArgs &a, int k) {
+    constexpr int T = (1 << L) / E;
+    const float2 *row = a.y1t + (size_t)k * a.npad;
+#pragma unroll
+    for (int u = 0; u < E; ++u) {
+        const int j = threadIdx.x + T * u;
+        x[u] = j < a.n ? __ldcs(row + j) : make_float2(0.f, 0.f);
+    }
+}
+
+template <int L, int E>
+__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4) k_af_entropy(AfRangeArgs a) {
+    using F = F32Fft<L, E>;
+    constexpr int T = F::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2 *xbuf = reinterpret_cast<float2 *>(smem);
+    __shared__ double red[2][32];
+    const int tid = threadIdx.x;
+    float2 x[E];
+    af_load_range_row<L, E>(x, a, blockIdx.x);
+    F::run(x, xbuf, a.tw, tid);
+    double s = 0.0, h = 0.0;
+#pragma unroll
+    for (int v = 0; v < E; ++v) {
+        const float in = fmaf(x[v].x, x[v].x, x[v].y * x[v].y);
+        s += in;
+        if (in > 0.f) h += (double)in * (double)logf(in);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        h += __shfl_xor_sync(0xffffffffu, h, o);
+    }
+    if ((tid & 31) == 0) { red[0][tid >> 5] = s; red[1][tid >> 5] = h; }
+    __syncthreads();
+    if (tid == 0) {
+        double ss = 0.0, hh = 0.0;
+        for (int w = 0; w < T / 32; ++w) { ss += red[0][w]; hh += red[1][w]; }
+        atomicAdd(a.acc, ss);
+        atomicAdd(a.acc + 1, hh);
+    }
+}
+
+template <int L, int E>
+__global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4)
+k_af_range_adjoint(AfRangeArgs a) {
+    namespace cg = cooperative_groups;
+    using F = F32Fft<L, E>;
+    constexpr int N = F::N, T = F::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2 *xbuf = reinterpret_cast<float2 *>(smem);
+    cg::cluster_group cluster = cg::this_cluster();
+    const int tid = threadIdx.x;
+    const int k = blockIdx.x;                         // cross bin
+    const double S = a.acc[0];
+    const double Ent = log(S) - a.acc[1] / S;
+    const float invS = (float)(1.0 / S), off = (float)(Ent - log(S));
+    float2 x[E];
+    af_load_range_row<L, E>(x, a, k);
+    F::run(x, xbuf, a.tw, tid);                       // recompute z along range
+#pragma unroll
+    for (int v = 0; v < E; ++v) {
+        const float in = fmaf(x[v].x, x[v].x, x[v].y * x[v].y);
+        const float c = in > 0.f ? -invS * (logf(in) + off) : 0.f;     // dE/dI
+        x[v] = make_float2(c * x[v].x, -c * x[v].y);                    // conj(g_z)
+    }
+    F::run(x, xbuf, a.tw, tid);                       // F^H g = conj(F conj(g))
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < E; ++v) xbuf[tid + T * v] = make_float2(x[v].x, -x[v].y);   // range index j
+    cluster.sync();
+    const int rank = (int)cluster.block_rank();
+    const int k0 = k - rank;
+    constexpr int SLICE = N / kCT;
+#pragma unroll
+    for (int s2 = 0; s2 < E; ++s2) {
+        const int item = tid + T * s2;
+        const int r = item % kCT;
+        const int j = rank * SLICE + item / kCT;
+        if (j < a.n) {
+            const float2 *remote = cluster.map_shared_rank(xbuf, r);
+            a.zadj_t[(size_t)j * a.m2 + k0 + r] = remote[j];
+        }
+    }
+    cluster.sync();
+}
+
+struct AfCrossArgs {
+    const float2 *zadj_t;   // [n][m2]
+    const float2 *p1;       // [n][mpad] forward pass-1 output (phase corrected)
+    const double *tan_s, *kr_grid, *kc_grid, *ham_m, *ham_n;
+    const float2 *tw;       // cross twiddles (m2)
+    float *dacc;            // [mpad] per-slot Im sum conj(g_p1) p1
+    int m, n, mpad, window;
+};
+
+// packed pass-2 bracket: bit 31 = outside the span, bits 17..30 = lower index, bits 0..16 = weight
+__device__ __forceinline__ uint32_t pack_br(int dead, int lowi, float f) {
+    const uint32_t q = (uint32_t)fminf(fmaxf(rintf(f * 131071.f), 0.f), 131071.f);
+    return ((uint32_t)dead << 31) | ((uint32_t)lowi << 17) | q;
+}
+__device__ __forceinline__ int br_low(uint32_t p) { return (int)((p >> 17) & 0x3fffu); }
+__device__ __forceinline__ float br_w(uint32_t p) { return (float)(p & 0x1ffffu) * (1.0f / 131071.f); }
+
+template <int L, int E>
+__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4) k_af_cross_adjoint(AfCrossArgs a) {
+    using F = F32Fft<L, E>;
+    constexpr int N = F::N, T = F::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2 *xbuf = reinterpret_cast<float2 *>(smem);
+    uint32_t *pk = reinterpret_cast<uint32_t *>(smem + (size_t)8 * F::xbuf_elems());
+    const int tid = threadIdx.x;
+    const int j = blockIdx.x;                         // range bin (< n)
+    const int m = a.m;
+    // forward pass-2 brackets of this range bin (ascending source axis: KR[j] > 0)
+    const double krj = a.kr_grid[j];
+    const double lo_v = krj * a.tan_s[0], hi_v = krj * a.tan_s[m - 1];
+    auto xa = [&](int t) { return krj * __ldg(a.tan_s + t); };
+    const double inv_span = (double)(m - 1) / (hi_v - lo_v);
+    for (int k = tid; k < m; k += T) {
+        const double q = a.kc_grid[k];
+        Frac fr{0.f, 0, 0};
+        const int g = isfinite(inv_span) ? (int)((q - lo_v) * inv_span) : 0;
+        const int ja = interp_bracket<false>(xa, m, lo_v, hi_v, q, g, fr);
+        pk[k] = ja >= 0 ? pack_br(0, ja, fr.f) : pack_br(1, q < lo_v ? 0 : m - 2, 0.f);
+    }
+    // adjoint of the cross FFT
+    const float2 *row = a.zadj_t + (size_t)j * N;
+    float2 x[E];
+#pragma unroll
+    for (int u = 0; u < E; ++u) {
+        const float2 v = __ldcs(row + tid + T * u);
+        x[u] = make_float2(v.x, -v.y);
+    }
+    F::run(x, xbuf, a.tw, tid);
+    const double hn = a.window ? a.ham_n[j] : 1.0;
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < E; ++v) {
+        const int k = tid + T * v;
+        float w = 0.f;
+        if (k < m) w = a.window ? (float)(a.ham_m[k] * hn) : 1.0f;
+        xbuf[k] = make_float2(w * x[v].x, -w * x[v].y);      // W . F_cross^H g, cross index k
+    }
+    __syncthreads();
+    // R2^H, atomics free: slot r collects bracket k with lower index r (weight 1-f) and r-1 (weight f);
+    // the lower index is monotone in k, so each thread walks one contiguous run of k for its 16 slots
+    const int r_lo = tid * E;
+    if (r_lo < m) {
+        int lo = 0, hi = m;                             // first k with lower index >= r_lo - 1
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (br_low(pk[mid]) < r_lo - 1) lo = mid + 1; else hi = mid;
+        }
+        int kp = lo;
+        const float2 *p1row = a.p1 + (size_t)j * a.mpad;
+#pragma unroll 1
+        for (int s2 = 0; s2 < E; ++s2) {
+            const int r = r_lo + s2;
+            if (r >= m) break;
+            float2 gsum = make_float2(0.f, 0.f);
+            for (int kk = kp; kk < m; ++kk) {
+                const uint32_t b = pk[kk];
+                const int l = br_low(b);
+                if (l > r) break;
+                if (b >> 31) continue;
+                const float f = br_w(b);
+                const float wgt = (l == r) ? 1.0f - f : (l == r - 1 ? f : 0.f);
+                const float2 y = xbuf[kk];
+                gsum.x = fmaf(wgt, y.x, gsum.x);
+                gsum.y = fmaf(wgt, y.y, gsum.y);
+            }
+            while (kp < m && br_low(pk[kp]) < r) ++kp;
+            const float2 pv = p1row[r];
+            atomicAdd(a.dacc + r, gsum.x * pv.y - gsum.y * pv.x);   // Im(conj(g) p1)
+        }
+    }
+}
+
+__global__ void k_af_finish(const float *dacc, const int32_t *order, const double *acc, float *dtheta, double *ent, int m) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < m) dtheta[order[r]] = 2.0f * dacc[r];
+    if (r == 0 && ent) ent[0] = log(acc[0]) - acc[1] / acc[0];
+}
+
 // ------------------------------------------------------------------------------------------ launch
 template <int L>
 struct Cfg {
@@ -508,6 +718,7 @@ cudaError_t float_alloc(FloatDev &d, int m, int n) {
 void float_free(FloatDev &d) {
     dfr(d.f0); dfr(d.df); dfr(d.flast); dfr(d.pr); dfr(d.tan_s); dfr(d.order); dfr(d.kr); dfr(d.kc); dfr(d.ham_m64);
     dfr(d.ham_n64); dfr(d.twm); dfr(d.twn); dfr(d.tabf); dfr(d.p1); dfr(d.y1);
+    dfr(d.af_zadj); dfr(d.af_acc); dfr(d.af_dacc);
 }
 
 cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int detect, cudaStream_t st, StageProf *prof) {
@@ -516,7 +727,7 @@ cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int dete
     pf.count = 0;
     cudaError_t e = pf.mark(st, "start");
     if (e != cudaSuccess) return e;
-    FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabf, d.p1, d.m, d.n, d.mpad};
+    FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabf, nullptr, d.p1, d.m, d.n, d.mpad};
     dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + F1_BINS - 1) / F1_BINS);
     if (d.range_sinc) {
         e = cudaFuncSetAttribute(k_fl_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1_smem(true));
@@ -536,6 +747,95 @@ cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int dete
     e = dispatch_fft2(d, out, detect, scale, st);
     if (e != cudaSuccess) return e;
     return pf.mark(st, "fft2_detect");
+}
+
+template <int L>
+cudaError_t launch_af_range(const FloatDev &d, cudaStream_t st) {
+    using F = F32Fft<L, Cfg<L>::E>;
+    AfRangeArgs p{d.y1, d.twn, d.af_acc, d.af_zadj, d.n, d.npad, d.m2};
+    const size_t sm = (size_t)8 * F::xbuf_elems();
+    auto f1 = k_af_entropy<L, Cfg<L>::E>;
+    auto f2 = k_af_range_adjoint<L, Cfg<L>::E>;
+    cudaError_t e = cudaFuncSetAttribute(f1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    f1<<<d.m2, Cfg<L>::T, sm, st>>>(p);
+    f2<<<d.m2, Cfg<L>::T, sm, st>>>(p);
+    return cudaGetLastError();
+}
+
+template <int L>
+cudaError_t launch_af_cross(const FloatDev &d, cudaStream_t st) {
+    using F = F32Fft<L, Cfg<L>::E>;
+    AfCrossArgs p{d.af_zadj, d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.twm, d.af_dacc, d.m, d.n, d.mpad, d.window};
+    const size_t sm = (size_t)8 * F::xbuf_elems() + (size_t)4 * d.m;
+    auto fn = k_af_cross_adjoint<L, Cfg<L>::E>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    fn<<<d.n, Cfg<L>::T, sm, st>>>(p);
+    return cudaGetLastError();
+}
+
+#define PFA_DISPATCH_L(Lv, call)                                        \
+    switch (Lv) {                                                       \
+        case 6: return call<6>; case 7: return call<7>;                 \
+        case 8: return call<8>; case 9: return call<9>;                 \
+        case 10: return call<10>; case 11: return call<11>;             \
+        case 12: return call<12>; case 13: return call<13>;             \
+        default: return cudaErrorInvalidValue;                          \
+    }
+
+cudaError_t af_range(const FloatDev &d, cudaStream_t st) {
+#define CALL(Lx) launch_af_range<Lx>(d, st)
+    switch (d.Ln) {
+        case 6: return CALL(6); case 7: return CALL(7); case 8: return CALL(8); case 9: return CALL(9);
+        case 10: return CALL(10); case 11: return CALL(11); case 12: return CALL(12); case 13: return CALL(13);
+        default: return cudaErrorInvalidValue;
+    }
+#undef CALL
+}
+
+cudaError_t af_cross(const FloatDev &d, cudaStream_t st) {
+#define CALL(Lx) launch_af_cross<Lx>(d, st)
+    switch (d.Lm) {
+        case 6: return CALL(6); case 7: return CALL(7); case 8: return CALL(8); case 9: return CALL(9);
+        case 10: return CALL(10); case 11: return CALL(11); case 12: return CALL(12); case 13: return CALL(13);
+        default: return cudaErrorInvalidValue;
+    }
+#undef CALL
+}
+#undef PFA_DISPATCH_L
+
+// Entropy and its gradient w.r.t. the per-pulse phase correction theta (float32, lerp passes).
+cudaError_t autofocus_grad(const FloatDev &d0, const float2 *sig, const float *theta, float *dtheta, double *ent,
+                           cudaStream_t st, StageProf *prof) {
+    StageProf none;
+    StageProf &pf = prof ? *prof : none;
+    pf.count = 0;
+    cudaError_t e = pf.mark(st, "start");
+    if (e != cudaSuccess) return e;
+    FloatDev d = d0;
+    d.layout = PFA_LAYOUT_NATURAL;      // |z| (so E) does not depend on the centring
+    d.sgn = -1;
+    if ((e = cudaMemsetAsync(d.af_acc, 0, 2 * sizeof(double), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(d.af_dacc, 0, sizeof(float) * d.mpad, st)) != cudaSuccess) return e;
+    FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabf, theta, d.p1, d.m, d.n, d.mpad};
+    dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + F1_BINS - 1) / F1_BINS);
+    e = cudaFuncSetAttribute(k_fl_pass1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1_smem(false));
+    if (e != cudaSuccess) return e;
+    k_fl_pass1<false><<<g1, 256, f1_smem(false), st>>>(p1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = pf.mark(st, "pass1_phase")) != cudaSuccess) return e;
+    if ((e = dispatch_pass2<false>(d, st)) != cudaSuccess) return e;
+    if ((e = pf.mark(st, "pass2_win_fft1")) != cudaSuccess) return e;
+    if ((e = af_range(d, st)) != cudaSuccess) return e;
+    if ((e = pf.mark(st, "range_entropy_adjoint")) != cudaSuccess) return e;
+    if ((e = af_cross(d, st)) != cudaSuccess) return e;
+    if ((e = pf.mark(st, "cross_adjoint_pass2T")) != cudaSuccess) return e;
+    k_af_finish<<<(d.m + 255) / 256, 256, 0, st>>>(d.af_dacc, d.order, d.af_acc, dtheta, ent, d.m);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return pf.mark(st, "finish");
 }
 
 }  // namespace pfa
@@ -573,6 +873,8 @@ pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *job) {
         const int r = job->order[i];
         if (r < 0 || r >= m || seen[r]++) return ffail(p, PFA_ERR_BAD_ARG, "order is not a permutation");
     }
+    d.kr_positive = 1;
+    for (int j = 0; j < n; ++j) if (!(job->kr_grid[j] > 0.0)) d.kr_positive = 0;
     d.sgn = job->sgn < 0 ? -1 : 1;
     d.layout = job->layout;
     d.window = (job->ham_m && job->ham_n) ? 1 : 0;
@@ -636,6 +938,30 @@ pfa_status pfa_form_float_host(pfa_plan *p, const float *sig_host, void *out_hos
     if ((e = cudaMemcpyAsync(out_host, p->staging_out, out_b, cudaMemcpyDeviceToHost, p->host_stream)) != cudaSuccess)
         return fcuda(p, e, "d2h");
     if ((e = cudaStreamSynchronize(p->host_stream)) != cudaSuccess) return fcuda(p, e, "sync");
+    return PFA_OK;
+}
+
+pfa_status pfa_autofocus_grad(pfa_plan *p, const float *sig_dev, const float *theta_dev, float *dtheta_dev,
+                              double *entropy_dev, void *stream) {
+    if (!p || !sig_dev || !theta_dev || !dtheta_dev) return PFA_ERR_BAD_ARG;
+    if (p->cfg.mode != PFA_MODE_FLOAT32 && p->cfg.mode != PFA_MODE_MIXED) return ffail(p, PFA_ERR_BAD_CONFIG, "plan is not float mode");
+    if (!p->job_ready) return ffail(p, PFA_ERR_NOT_READY, "pfa_set_float_job not called");
+    pfa::FloatDev &d = p->fl;
+    if (d.range_sinc || d.az_sinc) return ffail(p, PFA_ERR_BAD_CONFIG, "autofocus gradient supports the lerp resampler");
+    if (!d.kr_positive) return ffail(p, PFA_ERR_BAD_CONFIG, "autofocus gradient needs positive KR (ascending pass-2 sources)");
+    if (reinterpret_cast<uintptr_t>(sig_dev) & 7) return ffail(p, PFA_ERR_BAD_ARG, "signal must be 8-byte aligned");
+    DevGuard dg(p->device);
+    cudaError_t e;
+    if (!d.af_zadj) {
+        if ((e = pfa::dal(&d.af_zadj, (size_t)d.n * d.m2)) != cudaSuccess ||
+            (e = pfa::dal(&d.af_acc, 2)) != cudaSuccess || (e = pfa::dal(&d.af_dacc, d.mpad)) != cudaSuccess) {
+            pfa::dfr(d.af_zadj); pfa::dfr(d.af_acc); pfa::dfr(d.af_dacc);
+            return fcuda(p, e, "autofocus workspace");
+        }
+    }
+    e = pfa::autofocus_grad(d, reinterpret_cast<const float2 *>(sig_dev), theta_dev, dtheta_dev, entropy_dev,
+                            reinterpret_cast<cudaStream_t>(stream), &p->prof);
+    if (e != cudaSuccess) return fcuda(p, e, "autofocus");
     return PFA_OK;
 }
 

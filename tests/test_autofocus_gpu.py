@@ -1,0 +1,60 @@
+"""GPU: the autofocus adjoint against an FP64 torch-autograd reference and central finite differences
+of the FP64 objective (tolerance 1e-3 relative, per the stated target), plus a focusing run."""
+import numpy as np
+import pytest
+
+from oracle import autofocus_ref as afr
+from pfa_b200 import autofocus, engine, geometry, synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _scene(m, n, seed):
+    sc = synth.make_scene(m, n, n_targets=8, clutter_db=-10.0, snr_db=20.0, seed=seed)
+    tb = geometry.prepare_tables_from_scene(sc)
+    phi = afr.phase_error(m, seed=seed)
+    sig = (sc.signal * np.exp(1j * phi)[:, None]).astype(np.complex64)
+    return sig, tb, phi
+
+
+@pytest.mark.parametrize("m,n,seed", [(128, 128, 4), (256, 256, 5), (200, 240, 6)])
+def test_gradient_matches_fp64_autograd(torch_cuda, m, n, seed):
+    torch = torch_cuda
+    sig, tb, phi = _scene(m, n, seed)
+    theta = np.random.default_rng(seed).normal(0.0, 0.3, m)
+    e64, g64 = afr.entropy_and_grad(sig, tb, theta)
+    with engine.FloatPlan(m, n) as plan:
+        plan.set_tables(tb)
+        ent, g = autofocus.entropy_grad(plan, torch.from_numpy(sig).cuda(),
+                                        torch.from_numpy(theta.astype(np.float32)).cuda())
+    g = g.cpu().numpy().astype(np.float64)
+    assert abs(float(ent) - e64) / abs(e64) < 1e-5
+    assert np.linalg.norm(g - g64) / np.linalg.norm(g64) < 1e-3
+    idx = [1, m // 3, m // 2, m - 2]
+    fd = afr.fd_grad(sig, tb, theta, idx)
+    assert np.abs(g[idx] - fd).max() / np.abs(fd).max() < 1e-3
+
+
+def test_autograd_function_and_focusing(torch_cuda):
+    torch = torch_cuda
+    sig, tb, phi = _scene(256, 256, 7)
+    x = torch.from_numpy(sig).cuda()
+    with engine.FloatPlan(256, 256) as plan:
+        plan.set_tables(tb)
+        th = torch.zeros(256, device="cuda", requires_grad=True)
+        e = autofocus.image_entropy(th, plan, x)
+        e.backward()
+        _, g = autofocus.entropy_grad(plan, x, torch.zeros(256, device="cuda"))
+        assert torch.allclose(th.grad, g)
+        theta, hist = autofocus.autofocus(plan, x, steps=50, step=0.3, history=True)
+    assert hist[-1] < hist[0]
+    e_true = afr.entropy(sig, tb, phi)
+    assert hist[-1] <= e_true + 0.1 * (hist[0] - e_true)
