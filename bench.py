@@ -152,6 +152,71 @@ def stage_bytes(stage: str, m: int, n: int, G: int, mode: str = "fixed") -> floa
     }[stage]
 
 
+def _device_ms(fn, steps, warmup):
+    """Mean device time (ms) of fn() over `steps` calls after `warmup`, CUDA events on the current stream."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def measure_modes(a, local):
+    """The other configurations of the metric, device-timed at N=1: the NDSU-shaped float frame
+    (8167x8192 -> 8192^2; FP32 lerp as form_image_pfa, FP32 32-tap sinc) and the image-entropy autofocus
+    gradient on the 4096^2 scene (grads/s)."""
+    import numpy as np
+    import torch
+    from pfa_b200 import autofocus, engine, geometry, synth
+    from oracle import autofocus_ref
+    steps = max(3, min(a.steps, 10))
+    out = {}
+    sc, sig = synth.make_scene_device(8167, 8192, device=f"cuda:{local}", **{k: v for k, v in synth.WORKLOADS["ndsu_8167x8192"].items() if k not in ("m", "n")})
+    tables = geometry.prepare_tables_from_scene(sc)
+    for name, rs in (("float_fp32_lerp", False), ("float_fp32_sinc", True)):
+        with engine.FloatPlan(8167, 8192, rs, rs, device=local) as plan:
+            plan.set_tables(tables)
+            img = torch.empty((8192, 8192), dtype=torch.float32, device=sig.device)
+            ms = _device_ms(lambda: plan.form(sig, out=img), steps, 3)
+            plan.set_profiling(True)
+            plan.form(sig, out=img)
+            st = plan.stage_times()
+            plan.set_profiling(False)
+        fb = sum(stage_bytes(s, 8167, 8192, 8192, "float") for s in st)
+        out[name] = {"workload": "ndsu_8167x8192 -> 8192^2", "ms_per_frame": round(ms, 4),
+                     "stages_ms": {k: round(v, 4) for k, v in st.items()},
+                     "frame_bytes": fb, "frame_frac_of_hbm": round(fb / (ms * 1e-3) / 1e9 / _peaks()[0], 4)}
+    del sig
+    wl = synth.WORKLOADS["autofocus_4096"]
+    sc, sig = synth.make_scene_device(4096, 4096, device=f"cuda:{local}", **{k: v for k, v in wl.items() if k not in ("m", "n")})
+    phi = torch.as_tensor(autofocus_ref.phase_error(4096, seed=4), device=sig.device)
+    sig = (sig * torch.polar(torch.ones_like(phi), phi)[:, None].to(torch.complex64)).contiguous()
+    tables = geometry.prepare_tables_from_scene(sc)
+    with engine.FloatPlan(4096, 4096, device=local) as plan:
+        plan.set_tables(tables)
+        theta = torch.zeros(4096, dtype=torch.float32, device=sig.device)
+        dth = torch.empty_like(theta)
+        ent = torch.empty((), dtype=torch.float64, device=sig.device)
+        ms = _device_ms(lambda: autofocus.entropy_grad(plan, sig, theta, dth, ent), steps, 3)
+        plan.set_profiling(True)
+        autofocus.entropy_grad(plan, sig, theta, dth, ent)
+        st = plan.stage_times()
+        plan.set_profiling(False)
+        _, hist = autofocus.autofocus(plan, sig, steps=50, step=0.3, history=True)
+    out["autofocus_4096"] = {"workload": "4096x4096 c64, 128 targets + clutter, quadratic 3 rad + random walk "
+                                         "0.05 rad/pulse phase error; entropy gradient w.r.t. 4096 phases",
+                             "ms_per_grad": round(ms, 4), "grads_per_s": round(1000.0 / ms, 1),
+                             "stages_ms": {k: round(v, 4) for k, v in st.items()},
+                             "entropy_first_last_of_50_steps": [round(hist[0], 5), round(hist[-1], 5)]}
+    return out
+
+
 def run_ours(a, ws, rank, local):
     import numpy as np
     import torch
@@ -284,6 +349,8 @@ def run_ours(a, ws, rank, local):
         "cpu_baseline": cpu,
     }
     plan.close()
+    if ws == 1 and not a.no_modes:
+        line["modes"] = measure_modes(a, local)
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -342,6 +409,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=512)
     ap.add_argument("--ref-sample", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-modes", action="store_true", help="skip the float and autofocus configurations")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     ws, rank, local = _dist()

@@ -43,10 +43,11 @@ class Scene:
     sgn: int = -1
     targets: np.ndarray | None = None    # (P, 2) x, y metres
     amps: np.ndarray | None = None       # (P,) complex
+    mn: tuple | None = None              # (M, N), also when the signal lives elsewhere
 
     @property
     def dims(self):
-        return self.signal.shape
+        return self.mn if self.mn is not None else self.signal.shape
 
 
 def _look_vectors(apc, srp, uiax, uiay):
@@ -104,7 +105,58 @@ def make_scene(m: int, n: int, *, fc: float = 9.6e9, bw: float = 600e6, aperture
             sig = sig + s * (rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n)))
         sig = sig.astype(np.complex64)
     return Scene(signal=sig, tx=apc.copy(), rcv=apc.copy(), srp=srp, sc0=sc0, scss=scss,
-                 uiax=uiax, uiay=uiay, sgn=-1, targets=tgt, amps=amp)
+                 uiax=uiax, uiay=uiay, sgn=-1, targets=tgt, amps=amp, mn=(m, n))
+
+
+def make_scene_device(m: int, n: int, device="cuda", **kw) -> tuple:
+    """Same scene model as ``make_scene`` (PVP from NumPy, so the tables are identical), with the
+    point-target sum, clutter and noise evaluated by torch on ``device`` in float64.  For benchmark
+    inputs of production size; parity fixtures use ``make_scene``.  Returns (Scene without signal,
+    complex64 device tensor)."""
+    import torch
+    sc = make_scene(m, n, with_signal=False, **kw)
+    dev = torch.device(device)
+    ax, ay = _look_vectors(sc.tx, sc.srp, sc.uiax, sc.uiay)
+    g = torch.Generator(device=dev).manual_seed(int(kw.get("seed", 0)) + 7919)
+    tgt = torch.as_tensor(sc.targets, device=dev)
+    amp = torch.as_tensor(sc.amps, device=dev)
+    out = torch.empty((m, n), dtype=torch.complex64, device=dev)
+    axd = torch.as_tensor(ax, device=dev)
+    ayd = torch.as_tensor(ay, device=dev)
+    sc0 = torch.as_tensor(sc.sc0, device=dev)
+    scss = torch.as_tensor(sc.scss, device=dev)
+    blk = 64
+    nq = (n + blk - 1) // blk
+    qq = torch.arange(nq, device=dev, dtype=torch.float64) * blk
+    rr = torch.arange(blk, device=dev, dtype=torch.float64)
+    npt = max(tgt.shape[0], 1)
+    chunk = max(1, (1 << 27) // (npt * (nq + blk)))
+    p_t = 0.0
+    for i0 in range(0, m, chunk):
+        i1 = min(m, i0 + chunk)
+        proj = axd[i0:i1, None] * tgt[None, :, 0] + ayd[i0:i1, None] * tgt[None, :, 1]        # (b, P)
+        ph0 = (4.0 * math.pi / C) * sc0[i0:i1, None] * proj
+        dph = (4.0 * math.pi / C) * scss[i0:i1, None] * proj
+        # s[i, 64 q + r] = sum_p (a_p e^{j(ph0 + 64 q dph)}) e^{j r dph}: one batched matmul per chunk
+        pa = ph0[:, None, :] + qq[None, :, None] * dph[:, None, :]                             # (b, Q, P)
+        a = (torch.polar(torch.ones_like(pa), pa) * amp[None, None, :]).to(torch.complex64)
+        pb = dph[:, :, None] * rr[None, None, :]                                               # (b, P, 64)
+        b = torch.polar(torch.ones_like(pb), pb).to(torch.complex64)
+        s = torch.bmm(a, b).reshape(i1 - i0, nq * blk)[:, :n]
+        out[i0:i1] = s
+        p_t += float((s.abs().double() ** 2).sum())
+    p_t /= m * n
+    clutter_db, snr_db = kw.get("clutter_db"), kw.get("snr_db", 20.0)
+    extra = 0.0
+    if clutter_db is not None:
+        extra += p_t * 10.0 ** (clutter_db / 10.0)
+    if snr_db is not None:
+        extra += (p_t + (p_t * 10.0 ** (clutter_db / 10.0) if clutter_db is not None else 0.0)) * 10.0 ** (-snr_db / 10.0)
+    if extra > 0.0:
+        sd = math.sqrt(extra / 2.0)
+        out += torch.complex(torch.randn((m, n), generator=g, device=dev) * sd,
+                             torch.randn((m, n), generator=g, device=dev) * sd)
+    return sc, out
 
 
 def _point_targets(ax, ay, sc0, scss, n, tgt, amp, blk: int = 64, pulse_chunk: int = 128):
@@ -167,7 +219,7 @@ class FakeReader:
         self.cphd_meta = type("Meta", (), {"Global": glob, "SceneCoordinates": scoords})()
 
     def get_data_size_as_tuple(self):
-        return (self.scene.signal.shape,)
+        return (tuple(self.scene.dims),)
 
     def read_pvp_variable(self, name, index=0):
         return {"TxPos": self.scene.tx, "RcvPos": self.scene.rcv, "SRPPos": self.scene.srp,
