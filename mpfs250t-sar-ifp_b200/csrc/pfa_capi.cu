@@ -231,8 +231,10 @@ pfa_status pfa_set_fixed_job(pfa_plan *p, const pfa_fixed_job *job) {
             tws[(1 << b) - 1 + k] = (uint32_t)(uint16_t)tw2[2 * src] | ((uint32_t)(uint16_t)tw2[2 * src + 1] << 16);
         }
     }
-    std::vector<int16_t> sinc(256 * 32);
-    if (job->sinc_q15) std::memcpy(sinc.data(), job->sinc_q15, sizeof(int16_t) * 256 * 32); else pfa::build_sinc_table(sinc.data());
+    std::vector<int16_t> sinc_pt(256 * 32), sinc(256 * 32);
+    if (job->sinc_q15) std::memcpy(sinc_pt.data(), job->sinc_q15, sizeof(int16_t) * 256 * 32); else pfa::build_sinc_table(sinc_pt.data());
+    for (int ph = 0; ph < 256; ++ph)          // device layout [tap][phase]
+        for (int t = 0; t < 32; ++t) sinc[t * 256 + ph] = sinc_pt[ph * 32 + t];
     cudaError_t e;
 #define CPY(dst, src, cnt) do { e = cudaMemcpy(dst, src, sizeof(*(dst)) * (cnt), cudaMemcpyHostToDevice); \
         if (e != cudaSuccess) return cuda_fail(p, e, "job upload"); } while (0)

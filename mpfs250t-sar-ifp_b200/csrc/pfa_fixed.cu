@@ -112,12 +112,12 @@ __device__ __forceinline__ uint32_t sinc_gather(const uint32_t *win, int base, i
                                                 const int16_t *tab) {
     if (b.idx < 0) return 0u;
     if (b.idx >= -kSincFirst && b.idx <= sn - (kSincTaps + kSincFirst)) {
-        const int16_t *c = tab + (b.wq >> 7) * kSincTaps;
+        const int16_t *c = tab + (b.wq >> 7);           // table stored [tap][phase]: phases spread over banks
         const uint32_t *x = win + (b.idx + kSincFirst - base);
         long long ar = 0, ai = 0;
 #pragma unroll
         for (int t = 0; t < kSincTaps; ++t) {
-            const int ct = c[t];
+            const int ct = c[t * 256];
             const uint32_t v = x[t];
             ar += (long long)(ct * 1) * lo16(v);
             ai += (long long)(ct * 1) * hi16(v);

@@ -121,12 +121,12 @@ __device__ __forceinline__ float2 gather_f32(const float2 *src, int base, int sn
     if (j < 0) return make_float2(0.f, 0.f);
     const float frac = fr.f;
     if (SINC && j >= 15 && j <= sn - 17) {
-        const float *c = tab + fr.ph * 32;
+        const float *c = tab + fr.ph;                    // table stored [tap][phase]: phases spread over banks
         const float2 *x = src + (j - 15 - base);
         float ar = 0.f, ai = 0.f;
 #pragma unroll
         for (int t = 0; t < 32; ++t) {
-            const float ct = fr.rev ? c[31 - t] : c[t];
+            const float ct = fr.rev ? c[(31 - t) * 256] : c[t * 256];
             ar = fmaf(ct, x[t].x, ar);
             ai = fmaf(ct, x[t].y, ai);
         }
@@ -883,7 +883,7 @@ pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *job) {
     pfa::full_twiddles(d.n2, twn);
     std::vector<float> tabf(256 * 32);
     const int16_t *tq = pfa::builtin_sinc_table();
-    for (int i = 0; i < 256 * 32; ++i) tabf[i] = (float)tq[i] / 32768.0f;
+    for (int i = 0; i < 256 * 32; ++i) tabf[(i & 31) * 256 + (i >> 5)] = (float)tq[i] / 32768.0f;   // [tap][phase]
     cudaError_t e;
 #define CPY(dst, src, cnt) do { e = cudaMemcpy(dst, src, sizeof(*(dst)) * (cnt), cudaMemcpyHostToDevice); \
         if (e != cudaSuccess) return fcuda(p, e, "float job upload"); } while (0)

@@ -49,7 +49,8 @@ struct NoAllocLayout {
     static constexpr size_t tw_raw = hamc + align256(4 * G);
     static constexpr size_t tw = tw_raw + align256(2 * G);
     static constexpr size_t sinc = tw + align256(4 * G);
-    static constexpr size_t e1 = sinc + align256(2 * 256 * 32);
+    static constexpr size_t sinc_raw = sinc + align256(2 * 256 * 32);
+    static constexpr size_t e1 = sinc_raw + align256(2 * 256 * 32);
     static constexpr size_t e2 = e1 + align256(4 * G);
     static constexpr size_t ctrl = e2 + align256(4 * G);
     static constexpr size_t p1 = ctrl + align256(4 * 16);
@@ -66,9 +67,11 @@ void *g_scratch_addr[kMaxDevices] = {};
 // Derived job vectors: the pass-1 source scale f32(f32(2 pr) / f32(c)), the slot -> pulse order and the
 // stage-contiguous twiddle table (stage b at offset 2^b - 1, entry k = raw[k << (L-1-b)]).
 __global__ void k_noalloc_prep(const float *__restrict__ pr, const int32_t *__restrict__ inv_order,
-                               const int16_t *__restrict__ tw_raw, float *__restrict__ fac,
-                               int32_t *__restrict__ order, uint32_t *__restrict__ tw, int m, int G, int L) {
+                               const int16_t *__restrict__ tw_raw, const int16_t *__restrict__ sinc_raw,
+                               float *__restrict__ fac, int32_t *__restrict__ order, uint32_t *__restrict__ tw,
+                               int16_t *__restrict__ sinc, int m, int G, int L) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 256 * 32) sinc[(i & 31) * 256 + (i >> 5)] = sinc_raw[i];    // [phase][tap] -> [tap][phase]
     if (i < m) {
         fac[i] = __fdiv_rn(__fmul_rn(2.0f, pr[i]), 299792458.0f);
         order[inv_order[i]] = i;   // inv_order was checked to be a permutation on the host
@@ -155,6 +158,7 @@ extern "C" pfa_status pfa_form_fixed_noalloc(const pfa_config *cfg, const pfa_fi
     float *pr = reinterpret_cast<float *>(base + Lt::pr);
     int32_t *inv = reinterpret_cast<int32_t *>(base + Lt::inv_order);
     int16_t *tw_raw = reinterpret_cast<int16_t *>(base + Lt::tw_raw);
+    int16_t *sinc_raw = reinterpret_cast<int16_t *>(base + Lt::sinc_raw);
 
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const int16_t *sinc = job->sinc_q15 ? job->sinc_q15 : pfa::builtin_sinc_table();
@@ -162,12 +166,14 @@ extern "C" pfa_status pfa_form_fixed_noalloc(const pfa_config *cfg, const pfa_fi
         {d.f0, job->f0, 4u * m}, {d.df, job->df, 4u * m}, {pr, job->pr, 4u * m}, {d.tan_s, job->tan_s, 4u * m},
         {inv, job->inv_order, 4u * m}, {d.krp, job->kr_grid, 4u * G}, {d.kcp, job->kc_grid, 4u * G},
         {d.hamr, job->ham_r, 4u * G}, {d.hamc, job->ham_c, 4u * G}, {tw_raw, job->twiddle, 2u * G},
-        {d.sinc, sinc, 2u * 256 * 32}};
+        {sinc_raw, sinc, 2u * 256 * 32}};
     for (const Cp &cp : cps) {
         if (cudaMemcpyAsync(cp.dst, cp.src, cp.bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) return PFA_ERR_CUDA;
     }
-    const int nthreads = (G - 1 > m ? G - 1 : m);
-    k_noalloc_prep<<<(nthreads + 255) / 256, 256, 0, st>>>(pr, inv, tw_raw, d.fac, d.order, d.tw, m, G, L);
+    int nthreads = (G - 1 > m ? G - 1 : m);
+    if (nthreads < 256 * 32) nthreads = 256 * 32;
+    k_noalloc_prep<<<(nthreads + 255) / 256, 256, 0, st>>>(pr, inv, tw_raw, sinc_raw, d.fac, d.order, d.tw, d.sinc,
+                                                           m, G, L);
     if (cudaGetLastError() != cudaSuccess) return PFA_ERR_CUDA;
     // fixed_form clears the reduction words (ctrl) itself before its first kernel
     if (pfa::fixed_form(d, sig_dev, nullptr, img_dev, st, nullptr) != cudaSuccess) return PFA_ERR_CUDA;
