@@ -214,7 +214,42 @@ def measure_modes(a, local):
                              "ms_per_grad": round(ms, 4), "grads_per_s": round(1000.0 / ms, 1),
                              "stages_ms": {k: round(v, 4) for k, v in st.items()},
                              "entropy_first_last_of_50_steps": [round(hist[0], 5), round(hist[-1], 5)]}
+    del sig
+    out["batch_16_uneven"] = measure_batch(a, local)
     return out
+
+
+def measure_batch(a, local, nscene=16, af_iters=5, streams=4):
+    """16 scenes with pulses and samples uniform in [2048, 8192] (seed 5), 64-512 targets + clutter, each
+    formed on its own pow2 raster after `af_iters` autofocus steps, autotuned FFT tiles; one CUDA graph
+    launch for the batch vs one scene at a time on one stream.  Aggregate frames/s."""
+    import numpy as np
+    import torch
+    from pfa_b200 import autotune, batch, geometry, synth
+    rng = np.random.default_rng(5)
+    scenes, tiles = [], []
+    for k in range(nscene):
+        m, n = (int(v) for v in rng.integers(2048, 8193, 2))
+        sc, x = synth.make_scene_device(m, n, device=f"cuda:{local}", n_targets=int(rng.integers(64, 513)),
+                                        clutter_db=-10.0, snr_db=20.0, seed=500 + k)
+        tb = geometry.prepare_tables_from_scene(sc)
+        tile, _ = autotune.tune_float(tb, x, reps=3)
+        scenes.append((tb, x))
+        tiles.append(tile)
+    bf = batch.BatchFormer(scenes, streams=streams, tiles=tiles, af_iters=af_iters, device=local)
+    bf.capture()
+    reps = max(2, min(a.steps, 5))
+    eager_ms = _device_ms(bf.run_eager, reps, 1)
+    graph_ms = _device_ms(bf.replay, reps, 1)
+    shapes = [list(map(int, s.shape)) for _, s in scenes]
+    bf.close()
+    return {"workload": f"{nscene} scenes, M,N uniform in [2048, 8192] (seed 5), 64-512 targets + clutter, "
+                        f"pow2 rasters, {af_iters} autofocus iterations each, FP32",
+            "shapes": shapes, "tiles": [list(t) for t in tiles], "streams": streams,
+            "graph_ms_per_batch": round(graph_ms, 3), "eager_ms_per_batch": round(eager_ms, 3),
+            "frames_per_s_graph": round(nscene * 1000.0 / graph_ms, 1),
+            "frames_per_s_one_at_a_time": round(nscene * 1000.0 / eager_ms, 1),
+            "speedup": round(eager_ms / graph_ms, 3)}
 
 
 def run_ours(a, ws, rank, local):

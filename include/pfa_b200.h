@@ -71,7 +71,10 @@ typedef struct pfa_config {
     int32_t range_interp;  /* pfa_interp for pass 1 (--range-sinc)                          */
     int32_t az_interp;     /* pfa_interp for pass 2 (--az-sinc)                             */
     int32_t device;        /* CUDA device ordinal                                           */
-    int32_t reserved[9];
+    int32_t fft_ept_cross; /* float: complex values per thread in the cross FFT (8 or 16; 0 = 16),
+                              i.e. CTA size pow2(m)/ept -- the tile shape the autotuner picks   */
+    int32_t fft_ept_range; /* float: same for the range FFT (pow2(n)/ept threads)               */
+    int32_t reserved[7];
 } pfa_config;
 
 /* Fixed-point job: host pointers, copied at pfa_set_fixed_job.  Built exactly as

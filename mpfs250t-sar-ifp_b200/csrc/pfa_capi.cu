@@ -161,6 +161,14 @@ pfa_status pfa_plan_create(const pfa_config *cfg, pfa_plan **out) {
         e = pfa::float_alloc(p->fl, c.m, c.n);
         p->fl.range_sinc = c.range_interp == PFA_INTERP_SINC;
         p->fl.az_sinc = c.az_interp == PFA_INTERP_SINC;
+        if ((c.fft_ept_cross != 0 && c.fft_ept_cross != 8 && c.fft_ept_cross != 16) ||
+            (c.fft_ept_range != 0 && c.fft_ept_range != 8 && c.fft_ept_range != 16)) {
+            pfa::float_free(p->fl);
+            delete p;
+            return PFA_ERR_BAD_CONFIG;
+        }
+        p->fl.ept_cross = c.fft_ept_cross == 8 ? 8 : 16;
+        p->fl.ept_range = c.fft_ept_range == 8 ? 8 : 16;
         p->ws_bytes = pfa::float_workspace_bytes(c.m, c.n);
         if (e == cudaErrorInvalidValue) { pfa::float_free(p->fl); delete p; return PFA_ERR_BAD_CONFIG; }
     } else {

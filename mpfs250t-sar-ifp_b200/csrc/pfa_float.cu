@@ -269,7 +269,7 @@ struct FPass2Args {
 constexpr int kCT = 8;
 
 template <int L, int E, bool SINC>
-__global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4)
+__global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((1 << L) / E >= 512) ? 2 : 4))
 k_fl_pass2_fft(FPass2Args a) {
     using F = F32Fft<L, E>;
     constexpr int N = F::N, T = F::T;
@@ -376,7 +376,7 @@ struct FFft2Args {
 };
 
 template <int L, int E>
-__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4) k_fl_fft2(FFft2Args a) {
+__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((1 << L) / E >= 512) ? 2 : 4)) k_fl_fft2(FFft2Args a) {
     using F = F32Fft<L, E>;
     constexpr int N = F::N, T = F::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -436,7 +436,7 @@ __device__ __forceinline__ void af_load_range_row(float2 (&x)[E], const AfRangeA
 }
 
 template <int L, int E>
-__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4) k_af_entropy(AfRangeArgs a) {
+__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((1 << L) / E >= 512) ? 2 : 4)) k_af_entropy(AfRangeArgs a) {
     using F = F32Fft<L, E>;
     constexpr int T = F::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -469,7 +469,7 @@ __global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4) k
 }
 
 template <int L, int E>
-__global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4)
+__global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((1 << L) / E >= 512) ? 2 : 4))
 k_af_range_adjoint(AfRangeArgs a) {
     namespace cg = cooperative_groups;
     using F = F32Fft<L, E>;
@@ -530,7 +530,7 @@ __device__ __forceinline__ int br_low(uint32_t p) { return (int)((p >> 17) & 0x3
 __device__ __forceinline__ float br_w(uint32_t p) { return (float)(p & 0x1ffffu) * (1.0f / 131071.f); }
 
 template <int L, int E>
-__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 512) ? 2 : 4) k_af_cross_adjoint(AfCrossArgs a) {
+__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((1 << L) / E >= 512) ? 2 : 4)) k_af_cross_adjoint(AfCrossArgs a) {
     using F = F32Fft<L, E>;
     constexpr int N = F::N, T = F::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -618,57 +618,75 @@ struct Cfg {
     static constexpr int T = N / E;
 };
 
-template <int L, bool SINC>
+template <int L, int E, bool SINC>
 cudaError_t launch_pass2(const FloatDev &d, cudaStream_t st) {
-    using F = F32Fft<L, Cfg<L>::E>;
+    using F = F32Fft<L, E>;
     FPass2Args p{d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabf,
                  d.twm, d.y1, d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0};
     size_t regA = (std::max((size_t)8 * d.m, (size_t)8 * F::xbuf_elems()) + 15) & ~(size_t)15;
     size_t sm = regA + (SINC ? 256 * 32 * 4 : 0);
-    auto fn = k_fl_pass2_fft<L, Cfg<L>::E, SINC>;
+    auto fn = k_fl_pass2_fft<L, E, SINC>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    fn<<<d.npad, Cfg<L>::T, sm, st>>>(p);
+    fn<<<d.npad, (1 << L) / E, sm, st>>>(p);
     return cudaGetLastError();
 }
 
-template <int L>
+template <int L, int E>
 cudaError_t launch_fft2(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st) {
-    using F = F32Fft<L, Cfg<L>::E>;
+    using F = F32Fft<L, E>;
     FFft2Args p{d.y1, d.twn, out, d.n, d.npad, d.layout == PFA_LAYOUT_CENTRED, detect, d.sgn > 0, scale};
     size_t sm = (size_t)8 * F::xbuf_elems();
-    auto fn = k_fl_fft2<L, Cfg<L>::E>;
+    auto fn = k_fl_fft2<L, E>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    fn<<<d.m2, Cfg<L>::T, sm, st>>>(p);
+    fn<<<d.m2, (1 << L) / E, sm, st>>>(p);
     return cudaGetLastError();
+}
+
+// FFT register tile: 16 complex values per thread by default, 8 on request (twice the CTA size) for
+// lines of 256 points and more
+template <int L, bool SINC>
+cudaError_t pass2_tile(const FloatDev &d, cudaStream_t st) {
+    if constexpr (L >= 8) {
+        if (d.ept_cross == 8) return launch_pass2<L, 8, SINC>(d, st);
+    }
+    return launch_pass2<L, Cfg<L>::E, SINC>(d, st);
+}
+
+template <int L>
+cudaError_t fft2_tile(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st) {
+    if constexpr (L >= 8) {
+        if (d.ept_range == 8) return launch_fft2<L, 8>(d, out, detect, scale, st);
+    }
+    return launch_fft2<L, Cfg<L>::E>(d, out, detect, scale, st);
 }
 
 template <bool SINC>
 cudaError_t dispatch_pass2(const FloatDev &d, cudaStream_t st) {
     switch (d.Lm) {
-        case 6: return launch_pass2<6, SINC>(d, st);
-        case 7: return launch_pass2<7, SINC>(d, st);
-        case 8: return launch_pass2<8, SINC>(d, st);
-        case 9: return launch_pass2<9, SINC>(d, st);
-        case 10: return launch_pass2<10, SINC>(d, st);
-        case 11: return launch_pass2<11, SINC>(d, st);
-        case 12: return launch_pass2<12, SINC>(d, st);
-        case 13: return launch_pass2<13, SINC>(d, st);
+        case 6: return pass2_tile<6, SINC>(d, st);
+        case 7: return pass2_tile<7, SINC>(d, st);
+        case 8: return pass2_tile<8, SINC>(d, st);
+        case 9: return pass2_tile<9, SINC>(d, st);
+        case 10: return pass2_tile<10, SINC>(d, st);
+        case 11: return pass2_tile<11, SINC>(d, st);
+        case 12: return pass2_tile<12, SINC>(d, st);
+        case 13: return pass2_tile<13, SINC>(d, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t dispatch_fft2(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st) {
     switch (d.Ln) {
-        case 6: return launch_fft2<6>(d, out, detect, scale, st);
-        case 7: return launch_fft2<7>(d, out, detect, scale, st);
-        case 8: return launch_fft2<8>(d, out, detect, scale, st);
-        case 9: return launch_fft2<9>(d, out, detect, scale, st);
-        case 10: return launch_fft2<10>(d, out, detect, scale, st);
-        case 11: return launch_fft2<11>(d, out, detect, scale, st);
-        case 12: return launch_fft2<12>(d, out, detect, scale, st);
-        case 13: return launch_fft2<13>(d, out, detect, scale, st);
+        case 6: return fft2_tile<6>(d, out, detect, scale, st);
+        case 7: return fft2_tile<7>(d, out, detect, scale, st);
+        case 8: return fft2_tile<8>(d, out, detect, scale, st);
+        case 9: return fft2_tile<9>(d, out, detect, scale, st);
+        case 10: return fft2_tile<10>(d, out, detect, scale, st);
+        case 11: return fft2_tile<11>(d, out, detect, scale, st);
+        case 12: return fft2_tile<12>(d, out, detect, scale, st);
+        case 13: return fft2_tile<13>(d, out, detect, scale, st);
         default: return cudaErrorInvalidValue;
     }
 }

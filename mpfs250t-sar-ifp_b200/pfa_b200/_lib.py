@@ -31,7 +31,7 @@ class PfaError(RuntimeError):
 class Config(C.Structure):
     _fields_ = [("mode", C.c_int32), ("m", C.c_int32), ("n", C.c_int32), ("grid", C.c_int32),
                 ("range_interp", C.c_int32), ("az_interp", C.c_int32), ("device", C.c_int32),
-                ("reserved", C.c_int32 * 9)]
+                ("fft_ept_cross", C.c_int32), ("fft_ept_range", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
 class FixedJob(C.Structure):

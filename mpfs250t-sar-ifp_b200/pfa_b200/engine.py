@@ -156,12 +156,14 @@ class FloatPlan(_Plan):
     DETECT = {"mag": _lib.DETECT_MAG, "power": _lib.DETECT_POWER, "complex": _lib.DETECT_COMPLEX}
 
     def __init__(self, m: int, n: int, range_sinc: bool = False, az_sinc: bool = False, mixed: bool = False,
-                 device: int = 0):
+                 device: int = 0, tile: tuple = (16, 16)):
+        """``tile``: complex values per thread of the (cross, range) FFTs, 8 or 16 (the autotuner's knob)."""
         cfg = _lib.Config(mode=_lib.MODE_MIXED if mixed else _lib.MODE_FLOAT32, m=m, n=n, grid=0,
                           range_interp=_lib.SINC if range_sinc else _lib.LERP,
-                          az_interp=_lib.SINC if az_sinc else _lib.LERP, device=device)
+                          az_interp=_lib.SINC if az_sinc else _lib.LERP, device=device,
+                          fft_ept_cross=int(tile[0]), fft_ept_range=int(tile[1]))
         super().__init__(cfg)
-        self.m, self.n, self.device = m, n, device
+        self.m, self.n, self.device, self.tile = m, n, device, tuple(tile)
         self.m2, self.n2 = geometry.pow2(m), geometry.pow2(n)
 
     def set_tables(self, tables: dict, window: bool = True, centred: bool = True):

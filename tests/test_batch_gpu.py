@@ -1,0 +1,89 @@
+"""GPU: FFT tile variants (the autotuner's knob), the autotuner, and batched uneven scenes in one
+CUDA graph against the one-scene-at-a-time path."""
+import numpy as np
+import pytest
+
+from oracle import float_pfa as fp
+from pfa_b200 import autotune, batch, engine, geometry, synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+@pytest.mark.parametrize("tile", [(8, 8), (8, 16), (16, 8)])
+def test_tile_variants_match_fp64(torch_cuda, tile):
+    sc = synth.make_scene(600, 900, n_targets=16, clutter_db=-10.0, snr_db=20.0, seed=61, jitter=0.3)
+    tb = geometry.prepare_tables_from_scene(sc)
+    with engine.FloatPlan(600, 900, tile=tile) as plan:
+        plan.set_tables(tb)
+        cz = plan.form(sc.signal, detect="complex")
+    r64 = fp.pfa_image(sc.signal, tb["freq"], tb["ax"], tb["ay"], tb["sgn"], precision="f64")
+    assert fp.rel_l2(cz, r64) <= 1e-6
+
+
+def test_autotuner_picks_a_candidate(torch_cuda, tmp_path, monkeypatch):
+    torch = torch_cuda
+    monkeypatch.setenv("PFA_TUNE_CACHE", str(tmp_path / "tune.json"))
+    autotune._MEM.clear()
+    sc = synth.make_scene(512, 1000, n_targets=8, seed=62)
+    tb = geometry.prepare_tables_from_scene(sc)
+    x = torch.from_numpy(sc.signal).cuda()
+    tile, times = autotune.tune_float(tb, x, reps=3)
+    assert tile in autotune.CANDIDATES and set(times) == set(autotune.CANDIDATES)
+    assert (tmp_path / "tune.json").is_file()
+    tile2, _ = autotune.tune_float(tb, x)           # cached
+    assert tile2 == tile
+
+
+def _scenes(torch, shapes, seed0):
+    out = []
+    for k, (m, n) in enumerate(shapes):
+        sc = synth.make_scene(m, n, n_targets=16, clutter_db=-10.0, snr_db=20.0, seed=seed0 + k)
+        out.append((geometry.prepare_tables_from_scene(sc), torch.from_numpy(sc.signal).cuda()))
+    return out
+
+
+def test_batch_graph_equals_one_at_a_time(torch_cuda):
+    torch = torch_cuda
+    scenes = _scenes(torch, [(300, 500), (700, 400), (1000, 900), (256, 256), (512, 700)], 70)
+    bf = batch.BatchFormer(scenes, streams=3, tiles=[(16, 16), (8, 16), (16, 8), (16, 16), (8, 8)])
+    bf.run_eager()
+    torch.cuda.synchronize()
+    eager = [im.clone() for im in bf.images]
+    for im in bf.images:
+        im.zero_()
+    bf.replay()
+    torch.cuda.synchronize()
+    for a, b in zip(eager, bf.images):
+        assert torch.equal(a, b)
+    # and each equals a stand-alone plan
+    for (tb, x), im in zip(scenes, bf.images):
+        with engine.FloatPlan(*x.shape) as p:
+            p.set_tables(tb)
+            ref = p.form(x)
+        assert fp.rel_l2(im.cpu().numpy(), ref.cpu().numpy()) <= 1e-6
+    bf.close()
+
+
+def test_batch_with_autofocus_iterations(torch_cuda):
+    torch = torch_cuda
+    scenes = _scenes(torch, [(256, 300), (400, 256), (300, 300)], 80)
+    bf = batch.BatchFormer(scenes, streams=2, af_iters=3)
+    bf.run_eager()
+    torch.cuda.synchronize()
+    eager = [im.clone() for im in bf.images]
+    th_eager = [t.clone() for t in bf.theta]
+    bf.replay()
+    torch.cuda.synchronize()
+    for a, b in zip(eager, bf.images):
+        assert fp.rel_l2(b.cpu().numpy(), a.cpu().numpy()) <= 1e-4
+    for a, b in zip(th_eager, bf.theta):
+        assert torch.allclose(a, b, atol=1e-4)
+    bf.close()
