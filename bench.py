@@ -285,18 +285,9 @@ def run_ours(a, ws, rank, local):
     plan.set_tables(tables)
     stream = torch.cuda.current_stream()
 
-    def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if ws == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from pfa_b200 import replicas
+    barrier = replicas.barrier
+    max_over_ranks = replicas.max_over_ranks
 
     for _ in range(a.warmup):
         plan.form(sig, out=img)
