@@ -137,6 +137,16 @@ pfa_status pfa_form_fixed_iq16(pfa_plan *plan, const int16_t *sig_iq_dev, uint16
 /* End-to-end host variant: copies the host signal in, forms, copies the image out, synchronises. */
 pfa_status pfa_form_fixed_host(pfa_plan *plan, const float *sig_host, uint16_t *img_host);
 
+/* Pipelined end-to-end frames from host memory, the counterpart of the reference's scene queue
+ * (sar_pipeline.watch -> process_scene, mpfs/host/sar_pipeline.py:118-163): nframes host signals in,
+ * nframes host images out.  Device staging is double buffered and uploads, frames and downloads run on
+ * three streams, so frame k+1's upload and frame k-1's download overlap frame k.  All frames share the
+ * plan's job (geometry).  Host buffers should be pinned for full PCIe bandwidth.  Synchronises. */
+pfa_status pfa_form_fixed_host_frames(pfa_plan *plan, const float *const *sig_hosts, uint16_t *const *img_hosts,
+                                      int32_t nframes);
+pfa_status pfa_form_float_host_frames(pfa_plan *plan, const float *const *sig_hosts, void *const *out_hosts,
+                                      int32_t detect, int32_t nframes);
+
 /* Allocation-free fixed-point frame, for callers that cannot allocate device memory: code running
  * where cudaMalloc is forbidden or unsafe (inside a host that owns all device memory through its own
  * pool, a real-time loop that must not hit the allocator, or a process whose allocator is already

@@ -195,6 +195,12 @@ pfa_status pfa_plan_destroy(pfa_plan *p) {
         if (p->staging_in) cudaFree(p->staging_in);
         if (p->staging_out) cudaFree(p->staging_out);
         if (p->host_stream) cudaStreamDestroy(p->host_stream);
+        for (cudaStream_t s : {p->pipe_up, p->pipe_comp, p->pipe_down}) if (s) cudaStreamDestroy(s);
+        for (int b = 0; b < 2; ++b) {
+            if (p->pipe_in[b]) cudaFree(p->pipe_in[b]);
+            if (p->pipe_out[b]) cudaFree(p->pipe_out[b]);
+        }
+        for (auto &ev : p->pipe_ev) if (ev) cudaEventDestroy(ev);
         for (auto &ev : p->prof.ev) if (ev) cudaEventDestroy(ev);
     }
     delete p;
@@ -316,6 +322,74 @@ pfa_status pfa_form_fixed_host(pfa_plan *p, const float *sig_host, uint16_t *img
     e = cudaStreamSynchronize(p->host_stream);
     if (e != cudaSuccess) return cuda_fail(p, e, "sync");
     return PFA_OK;
+}
+
+}  // extern "C"
+
+pfa_status pfa::run_host_frames(pfa_plan *p, const void *const *ins, void *const *outs, int32_t nframes,
+                                size_t in_b, size_t out_b, FrameFn form, int32_t arg) {
+    if (!ins || !outs || nframes < 0) return PFA_ERR_BAD_ARG;
+    for (int k = 0; k < nframes; ++k)
+        if (!ins[k] || !outs[k]) return PFA_ERR_BAD_ARG;
+    cudaError_t e;
+    for (cudaStream_t *s : {&p->pipe_up, &p->pipe_comp, &p->pipe_down})
+        if (!*s && (e = cudaStreamCreateWithFlags(s, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(p, e, "pipe stream");
+    for (auto &ev : p->pipe_ev)
+        if (!ev && (e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(p, e, "pipe event");
+    if (p->pipe_in_bytes < in_b || p->pipe_out_bytes < out_b) {
+        for (int b = 0; b < 2; ++b) {
+            if (p->pipe_in[b]) cudaFree(p->pipe_in[b]);
+            if (p->pipe_out[b]) cudaFree(p->pipe_out[b]);
+            p->pipe_in[b] = p->pipe_out[b] = nullptr;
+        }
+        p->pipe_in_bytes = p->pipe_out_bytes = 0;
+        for (int b = 0; b < 2; ++b) {
+            if ((e = cudaMalloc(&p->pipe_in[b], in_b)) != cudaSuccess) return cuda_fail(p, e, "pipe staging");
+            if ((e = cudaMalloc(&p->pipe_out[b], out_b)) != cudaSuccess) return cuda_fail(p, e, "pipe staging");
+        }
+        p->pipe_in_bytes = in_b;
+        p->pipe_out_bytes = out_b;
+    }
+    cudaEvent_t *uploaded = p->pipe_ev, *computed = p->pipe_ev + 2, *downloaded = p->pipe_ev + 4;
+    for (int k = 0; k < nframes; ++k) {
+        const int b = k & 1;
+        // upload k once frame k-2 no longer reads this staging buffer
+        if (k >= 2 && (e = cudaStreamWaitEvent(p->pipe_up, computed[b], 0)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+        if ((e = cudaMemcpyAsync(p->pipe_in[b], ins[k], in_b, cudaMemcpyHostToDevice, p->pipe_up)) != cudaSuccess)
+            return cuda_fail(p, e, "pipe h2d");
+        if ((e = cudaEventRecord(uploaded[b], p->pipe_up)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+        // frame k after its upload, and after frame k-2's image left this output buffer
+        if ((e = cudaStreamWaitEvent(p->pipe_comp, uploaded[b], 0)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+        if (k >= 2 && (e = cudaStreamWaitEvent(p->pipe_comp, downloaded[b], 0)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+        pfa_status st = form(p, p->pipe_in[b], p->pipe_out[b], p->pipe_comp, arg);
+        if (st != PFA_OK) return st;
+        if ((e = cudaEventRecord(computed[b], p->pipe_comp)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+        // download k
+        if ((e = cudaStreamWaitEvent(p->pipe_down, computed[b], 0)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+        if ((e = cudaMemcpyAsync(outs[k], p->pipe_out[b], out_b, cudaMemcpyDeviceToHost, p->pipe_down)) != cudaSuccess)
+            return cuda_fail(p, e, "pipe d2h");
+        if ((e = cudaEventRecord(downloaded[b], p->pipe_down)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+    }
+    for (cudaStream_t s : {p->pipe_up, p->pipe_comp, p->pipe_down})
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(p, e, "pipe sync");
+    return PFA_OK;
+}
+
+extern "C" {
+
+static pfa_status fixed_frame(pfa_plan *p, const void *in, void *out, cudaStream_t st, int32_t) {
+    return fixed_common(p, static_cast<const float *>(in), nullptr, static_cast<uint16_t *>(out), st);
+}
+
+pfa_status pfa_form_fixed_host_frames(pfa_plan *p, const float *const *sig_hosts, uint16_t *const *img_hosts,
+                                      int32_t nframes) {
+    if (!p) return PFA_ERR_BAD_ARG;
+    if (p->cfg.mode != PFA_MODE_FIXED) return fail(p, PFA_ERR_BAD_CONFIG, "plan is not fixed mode");
+    DeviceGuard dg(p->device);
+    const size_t in_b = sizeof(float) * 2 * (size_t)p->fx.m * p->fx.n;
+    const size_t out_b = sizeof(uint16_t) * (size_t)p->fx.G * p->fx.G;
+    return pfa::run_host_frames(p, reinterpret_cast<const void *const *>(sig_hosts),
+                                reinterpret_cast<void *const *>(img_hosts), nframes, in_b, out_b, fixed_frame, 0);
 }
 
 pfa_status pfa_get_fixed_exponents(pfa_plan *p, int32_t *e_range, int32_t *e_az, int32_t *q0_exp) {

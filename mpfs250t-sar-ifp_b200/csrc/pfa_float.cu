@@ -959,6 +959,22 @@ pfa_status pfa_form_float_host(pfa_plan *p, const float *sig_host, void *out_hos
     return PFA_OK;
 }
 
+static pfa_status float_frame(pfa_plan *p, const void *in, void *out, cudaStream_t st, int32_t detect) {
+    return pfa_form_float(p, static_cast<const float *>(in), out, detect, st);
+}
+
+pfa_status pfa_form_float_host_frames(pfa_plan *p, const float *const *sig_hosts, void *const *out_hosts,
+                                      int32_t detect, int32_t nframes) {
+    if (!p) return PFA_ERR_BAD_ARG;
+    if (p->cfg.mode != PFA_MODE_FLOAT32 && p->cfg.mode != PFA_MODE_MIXED) return ffail(p, PFA_ERR_BAD_CONFIG, "plan is not float mode");
+    if (detect < PFA_DETECT_MAG || detect > PFA_DETECT_COMPLEX) return ffail(p, PFA_ERR_BAD_ARG, "bad detect mode");
+    DevGuard dg(p->device);
+    const size_t in_b = sizeof(float) * 2 * (size_t)p->fl.m * p->fl.n;
+    const size_t out_b = (detect == PFA_DETECT_COMPLEX ? 8 : 4) * (size_t)p->fl.m2 * p->fl.n2;
+    return pfa::run_host_frames(p, reinterpret_cast<const void *const *>(sig_hosts), out_hosts, nframes, in_b, out_b,
+                                float_frame, detect);
+}
+
 pfa_status pfa_autofocus_grad(pfa_plan *p, const float *sig_dev, const float *theta_dev, float *dtheta_dev,
                               double *entropy_dev, void *stream) {
     if (!p || !sig_dev || !theta_dev || !dtheta_dev) return PFA_ERR_BAD_ARG;

@@ -79,6 +79,11 @@ struct pfa_plan {
     void *staging_out = nullptr;
     size_t staging_in_bytes = 0, staging_out_bytes = 0;
     cudaStream_t host_stream = nullptr;
+    // pipelined host frames: upload / compute / download streams, double-buffered staging
+    cudaStream_t pipe_up = nullptr, pipe_comp = nullptr, pipe_down = nullptr;
+    void *pipe_in[2] = {nullptr, nullptr}, *pipe_out[2] = {nullptr, nullptr};
+    size_t pipe_in_bytes = 0, pipe_out_bytes = 0;
+    cudaEvent_t pipe_ev[6] = {};      // uploaded[2], computed[2], downloaded[2]
     pfa::StageProf prof;
     std::string err;
 };
@@ -97,6 +102,11 @@ cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int dete
 size_t float_workspace_bytes(int m, int n);
 cudaError_t float_alloc(FloatDev &d, int m, int n);
 void float_free(FloatDev &d);
+
+// Pipelined host frames (pfa_capi.cu): form(plan, in_dev, out_dev, stream, arg) runs one frame.
+typedef pfa_status (*FrameFn)(pfa_plan *p, const void *in_dev, void *out_dev, cudaStream_t st, int32_t arg);
+pfa_status run_host_frames(pfa_plan *p, const void *const *ins, void *const *outs, int32_t nframes, size_t in_bytes,
+                           size_t out_bytes, FrameFn form, int32_t arg);
 
 // Host-side table builders used when the caller passes NULL for a table (libm based).
 void build_sinc_table(int16_t *tab);   // returns false-free: table from the exact-rational recipe

@@ -62,7 +62,9 @@ SIGNATURES = {
                                          C.c_void_p]),
     "pfa_form_float": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "pfa_form_float_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
-    "pfa_autofocus_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pfa_form_fixed_host_frames": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "pfa_form_float_host_frames": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
+    "pfa_autofocus_grad":(C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "pfa_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "pfa_get_stage_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_char_p, C.c_size_t]),
     "pfa_status_string": (C.c_char_p, [C.c_int]),

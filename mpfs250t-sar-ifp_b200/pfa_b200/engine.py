@@ -35,6 +35,19 @@ def _stream_handle(stream=None):
     return C.c_void_p(s.cuda_stream)
 
 
+def _frame_ptrs(arrays):
+    return (C.c_void_p * max(len(arrays), 1))(*[a.ctypes.data for a in arrays])
+
+
+def _checked_frames(arrays, shape, dtype, what):
+    """Host frames must be C-contiguous with the exact dtype/shape: the library writes through the raw
+    pointers, so a silent copy here would lose the caller's output (or its pinned input)."""
+    for a in arrays:
+        if not isinstance(a, np.ndarray) or a.dtype != dtype or a.shape != shape or not a.flags.c_contiguous:
+            raise ValueError(f"{what} frames must be C-contiguous {np.dtype(dtype).name} {shape}")
+    return list(arrays)
+
+
 class _Plan:
     def __init__(self, cfg: _lib.Config):
         self._lib = _lib.load()
@@ -140,6 +153,19 @@ class FixedPlan(_Plan):
         _lib.check(self._lib.pfa_form_fixed_host(self._h, _ptr(sig), _ptr(img)), self._h)
         return img
 
+    def form_host_frames(self, signals, outs=None):
+        """Pipelined end-to-end frames (pfa_form_fixed_host_frames): uploads, frames and downloads of
+        consecutive host frames overlap on three streams.  Pass pinned (page-locked) arrays for full
+        PCIe bandwidth.  Returns the list of (grid, grid) uint16 images."""
+        sigs = _checked_frames(signals, (self.m, self.n), np.complex64, "signal")
+        imgs = outs if outs is not None else [np.empty((self.grid, self.grid), np.uint16) for _ in sigs]
+        imgs = _checked_frames(imgs, (self.grid, self.grid), np.uint16, "image")
+        if len(imgs) != len(sigs):
+            raise ValueError("one output per signal")
+        _lib.check(self._lib.pfa_form_fixed_host_frames(self._h, _frame_ptrs(sigs), _frame_ptrs(imgs),
+                                                        len(sigs)), self._h)
+        return imgs
+
     def exponents(self):
         """(e_range[n], e_az[grid], q0_exp) of the last frame (fft_pass_bfp's per-row exponents)."""
         er = np.zeros(self.n, np.int32)
@@ -201,6 +227,18 @@ class FloatPlan(_Plan):
         _lib.check(self._lib.pfa_form_float_host(self._h, _ptr(sig), _ptr(img), self.DETECT[detect]), self._h)
         return img
 
+
+    def form_host_frames(self, signals, outs=None, detect: str = "mag"):
+        """Pipelined end-to-end frames (pfa_form_float_host_frames); see FixedPlan.form_host_frames."""
+        sigs = _checked_frames(signals, (self.m, self.n), np.complex64, "signal")
+        dt = np.complex64 if detect == "complex" else np.float32
+        imgs = outs if outs is not None else [np.empty((self.m2, self.n2), dt) for _ in sigs]
+        imgs = _checked_frames(imgs, (self.m2, self.n2), dt, "image")
+        if len(imgs) != len(sigs):
+            raise ValueError("one output per signal")
+        _lib.check(self._lib.pfa_form_float_host_frames(self._h, _frame_ptrs(sigs), _frame_ptrs(imgs),
+                                                        self.DETECT[detect], len(sigs)), self._h)
+        return imgs
 
 def focus_float(signal, tables, range_sinc=False, az_sinc=False, mixed=False, device=0):
     """Drop-in for ``accel.NumpyBackend.focus`` (mpfs/host/accel.py:39-44): float32 |img|."""
