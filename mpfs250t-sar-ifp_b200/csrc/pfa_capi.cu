@@ -157,7 +157,7 @@ pfa_status pfa_plan_create(const pfa_config *cfg, pfa_plan **out) {
         p->fx.range_sinc = c.range_interp == PFA_INTERP_SINC;
         p->fx.az_sinc = c.az_interp == PFA_INTERP_SINC;
         p->ws_bytes = pfa::fixed_workspace_bytes(c.m, c.n, c.grid);
-    } else if (c.mode == PFA_MODE_FLOAT32 || c.mode == PFA_MODE_MIXED) {
+    } else if (c.mode == PFA_MODE_FLOAT32) {
         e = pfa::float_alloc(p->fl, c.m, c.n);
         p->fl.range_sinc = c.range_interp == PFA_INTERP_SINC;
         p->fl.az_sinc = c.az_interp == PFA_INTERP_SINC;
