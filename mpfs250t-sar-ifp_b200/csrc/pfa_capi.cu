@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -16,6 +17,15 @@ namespace pfa {
 
 void build_sinc_table(int16_t *tab) { std::memcpy(tab, kSincQ15, sizeof(kSincQ15)); }
 const int16_t *builtin_sinc_table() { return kSincQ15; }
+bool sinc_table_fits_int32(const int16_t *tab) {
+    for (int ph = 0; ph < 256; ++ph)
+        for (int h = 0; h < 2; ++h) {
+            int s = 0;
+            for (int t = 16 * h; t < 16 * h + 16; ++t) s += std::abs((int)tab[ph * 32 + t]);
+            if (s > 65535) return false;
+        }
+    return true;
+}
 
 void build_twiddles_q15(int G, int16_t *tw2) {
     // floor(exp(-2 pi j k / G) * 32768) clipped to int16 (src/fixedpoint.py:277, quant mode 'trunc')
@@ -247,6 +257,8 @@ pfa_status pfa_set_fixed_job(pfa_plan *p, const pfa_fixed_job *job) {
     }
     std::vector<int16_t> sinc_pt(256 * 32), sinc(256 * 32);
     if (job->sinc_q15) std::memcpy(sinc_pt.data(), job->sinc_q15, sizeof(int16_t) * 256 * 32); else pfa::build_sinc_table(sinc_pt.data());
+    if (!pfa::sinc_table_fits_int32(sinc_pt.data()))
+        return fail(p, PFA_ERR_BAD_ARG, "sinc table: sum |tap| over a half of a phase exceeds 65535");
     for (int ph = 0; ph < 256; ++ph)          // device layout [tap][phase]
         for (int t = 0; t < 32; ++t) sinc[t * 256 + ph] = sinc_pt[ph * 32 + t];
     cudaError_t e;

@@ -114,14 +114,24 @@ __device__ __forceinline__ uint32_t sinc_gather(const uint32_t *win, int base, i
     if (b.idx >= -kSincFirst && b.idx <= sn - (kSincTaps + kSincFirst)) {
         const int16_t *c = tab + (b.wq >> 7);           // table stored [tap][phase]: phases spread over banks
         const uint32_t *x = win + (b.idx + kSincFirst - base);
-        long long ar = 0, ai = 0;
+        // Two int32 half sums (taps 0-15, 16-31): the table is checked on upload to have
+        // sum |tap| <= 65535 over each half of every phase, so |half sum| <= 32768 * 65535 < 2^31.
+        int ar0 = 0, ai0 = 0, ar1 = 0, ai1 = 0;
 #pragma unroll
-        for (int t = 0; t < kSincTaps; ++t) {
+        for (int t = 0; t < kSincTaps / 2; ++t) {
             const int ct = c[t * 256];
             const uint32_t v = x[t];
-            ar += (long long)(ct * 1) * lo16(v);
-            ai += (long long)(ct * 1) * hi16(v);
+            ar0 += ct * lo16(v);
+            ai0 += ct * hi16(v);
         }
+#pragma unroll
+        for (int t = kSincTaps / 2; t < kSincTaps; ++t) {
+            const int ct = c[t * 256];
+            const uint32_t v = x[t];
+            ar1 += ct * lo16(v);
+            ai1 += ct * hi16(v);
+        }
+        const long long ar = (long long)ar0 + ar1, ai = (long long)ai0 + ai1;
         return pack16((int)sat16ll((ar + (1 << 14)) >> 15), (int)sat16ll((ai + (1 << 14)) >> 15));
     }
     const uint32_t va = win[b.idx - base], vb = win[b.idx + 1 - base];
@@ -364,7 +374,8 @@ struct BfpFft {
                 if (b < done) continue;
                 // stage s = b + 1: pairs (p, p + 2^b); twiddle k = p mod 2^b from the stage table
                 const uint32_t *tws = tw + ((1 << b) - 1);
-                unsigned mx = 0;
+                // row max of |re|, |im| as max(largest, -smallest): no |.| per value
+                int hi = 0, lo_ = 0;
 #pragma unroll
                 for (int v = 0; v < E; ++v) {
                     if (v & (1 << rb)) continue;
@@ -380,12 +391,10 @@ struct BfpFft {
                     xi[v] = ai + ti;
                     xr[v2] = ar - tr;
                     xi[v2] = ai - ti;
+                    hi = __vimax3_s32(hi, __vimax3_s32(xr[v], xi[v], xr[v2]), xi[v2]);
+                    lo_ = __vimin3_s32(lo_, __vimin3_s32(xr[v], xi[v], xr[v2]), xi[v2]);
                 }
-#pragma unroll
-                for (int v = 0; v < E; ++v) {
-                    mx = max(mx, (unsigned)max(abs(xr[v]), abs(xi[v])));
-                }
-                mx = __reduce_max_sync(0xffffffffu, mx);
+                const unsigned mx = __reduce_max_sync(0xffffffffu, (unsigned)max(hi, -lo_));
                 if (lane == 0) red[rbuf][warp] = (int)mx;
                 __syncthreads();
                 int rowmax = 0;
@@ -395,11 +404,12 @@ struct BfpFft {
                 // max(0, ceil(log2((mx + 1) / 32767))) on integers
                 int sh = 0;
                 while ((long long)rowmax + 1 > (32767LL << sh)) ++sh;
+                // |x| <= rowmax < 32767 * 2^sh, so x >> sh lies in [-32767, 32766]: no saturation needed
                 if (sh) {
 #pragma unroll
                     for (int v = 0; v < E; ++v) {
-                        xr[v] = sat16(xr[v] >> sh);
-                        xi[v] = sat16(xi[v] >> sh);
+                        xr[v] >>= sh;
+                        xi[v] >>= sh;
                     }
                 }
                 e_row += sh;

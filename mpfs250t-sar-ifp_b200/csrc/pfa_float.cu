@@ -55,8 +55,22 @@ __device__ __forceinline__ int sinc_phase(double fd) {
     return (int)fmin(fmax(rint(fd * 32768.0), 0.0), 32767.0) >> 7;
 }
 
+// Fraction of x in [a, b].  EXACT: float64 fraction (the sinc phase depends on it); else a float32 division.
+template <bool EXACT>
+__device__ __forceinline__ void make_frac(double x, double a, double b, Frac &frac) {
+    if (EXACT) {
+        const double fd = __ddiv_rn(__dsub_rn(x, a), __dsub_rn(b, a));
+        frac.f = (float)fd;
+        frac.ph = sinc_phase(fd);
+    } else {
+        frac.f = __fdiv_rn((float)(x - a), (float)(b - a));
+        frac.ph = 0;
+    }
+    frac.rev = 0;
+}
+
 // Walks from the guess carrying both end values (two loads when the guess is right); bisection after a
-// few steps.  EXACT: float64 fraction (the sinc phase depends on it); else a float32 division.
+// few steps.
 template <bool EXACT, class F>
 __device__ __forceinline__ int interp_bracket(const F &xa, int n, double x0, double x1, double x, int guess, Frac &frac) {
     if (!(x >= x0) || !(x <= x1)) return -1;
@@ -96,16 +110,36 @@ __device__ __forceinline__ int interp_bracket(const F &xa, int n, double x0, dou
         b = a;
         a = xa(j);
     }
-    if (EXACT) {
-        const double fd = __ddiv_rn(__dsub_rn(x, a), __dsub_rn(b, a));
-        frac.f = (float)fd;
-        frac.ph = sinc_phase(fd);
-    } else {
-        frac.f = __fdiv_rn((float)(x - a), (float)(b - a));
-        frac.ph = 0;
-    }
-    frac.rev = 0;
+    make_frac<EXACT>(x, a, b, frac);
     return j;
+}
+
+// The same bracket for CH queries at once: every guess and both its end values are loaded before any is
+// tested, so the loads of the CH queries overlap; a query whose guess misses walks from it.
+template <bool EXACT, int CH, class F>
+__device__ __forceinline__ void interp_brackets(const F &xa, int n, double x0, double x1, double inv_span,
+                                                const double (&x)[CH], const bool (&valid)[CH], int (&j)[CH],
+                                                Frac (&frac)[CH]) {
+    int g[CH];
+    double a[CH], b[CH];
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+        g[c] = (valid[c] && isfinite(inv_span)) ? min(max((int)((x[c] - x0) * inv_span), 0), n - 2) : 0;
+        a[c] = xa(g[c]);
+        b[c] = xa(g[c] + 1);
+    }
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+        j[c] = -1;
+        frac[c] = Frac{0.f, 0, 0};
+        if (!valid[c] || !(x[c] >= x0) || !(x[c] <= x1)) continue;
+        if (a[c] <= x[c] && (x[c] < b[c] || g[c] == n - 2)) {
+            j[c] = g[c];
+            make_frac<EXACT>(x[c], a[c], b[c], frac[c]);
+        } else {
+            j[c] = interp_bracket<EXACT>(xa, n, x0, x1, x[c], g[c], frac[c]);
+        }
+    }
 }
 
 // the same bracket seen from the descending side: lower natural index n-2-j, weights mirrored
@@ -304,21 +338,30 @@ k_fl_pass2_fft(FPass2Args a) {
     const double hn = a.window ? a.ham_n[j] : 1.0;
     int bl[E];      // packed bracket: lower natural index | phase << 16 | reversed << 24; -1 = outside
     float bf[E];    // lerp weight toward the upper sample
+    constexpr int CH = 4;
 #pragma unroll
-    for (int u = 0; u < E; ++u) {
-        const int k = tid + T * u;
-        bl[u] = -1;
-        bf[u] = 0.f;
-        if (k < m) {
-            const double q = a.kc_grid[k];
-            Frac fr{0.f, 0, 0};
-            const int g = isfinite(inv_span) ? (int)((q - lo_v) * inv_span) : 0;
-            const int ja = interp_bracket<SINC>(xa, m, lo_v, hi_v, q, g, fr);
-            if (ja >= 0) {
-                int lowi = ja;
-                if (!asc) { lowi = m - 2 - ja; mirror_frac(fr); }
-                bl[u] = lowi | (fr.ph << 16) | (fr.rev << 24);
-                bf[u] = fr.f;
+    for (int u0 = 0; u0 < E; u0 += CH) {
+        double q[CH];
+        bool ok[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int k = tid + T * (u0 + c);
+            ok[c] = k < m;
+            q[c] = ok[c] ? __ldg(a.kc_grid + k) : 0.0;
+        }
+        int ja[CH];
+        Frac fr[CH];
+        interp_brackets<SINC, CH>(xa, m, lo_v, hi_v, inv_span, q, ok, ja, fr);
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int u = u0 + c;
+            bl[u] = -1;
+            bf[u] = 0.f;
+            if (ja[c] >= 0) {
+                int lowi = ja[c];
+                if (!asc) { lowi = m - 2 - ja[c]; mirror_frac(fr[c]); }
+                bl[u] = lowi | (fr[c].ph << 16) | (fr[c].rev << 24);
+                bf[u] = fr[c].f;
             }
         }
     }
@@ -544,12 +587,21 @@ __global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((
     const double lo_v = krj * a.tan_s[0], hi_v = krj * a.tan_s[m - 1];
     auto xa = [&](int t) { return krj * __ldg(a.tan_s + t); };
     const double inv_span = (double)(m - 1) / (hi_v - lo_v);
-    for (int k = tid; k < m; k += T) {
-        const double q = a.kc_grid[k];
-        Frac fr{0.f, 0, 0};
-        const int g = isfinite(inv_span) ? (int)((q - lo_v) * inv_span) : 0;
-        const int ja = interp_bracket<false>(xa, m, lo_v, hi_v, q, g, fr);
-        pk[k] = ja >= 0 ? pack_br(0, ja, fr.f) : pack_br(1, q < lo_v ? 0 : m - 2, 0.f);
+    constexpr int CH = 4;
+    for (int k0 = tid; k0 < m; k0 += CH * T) {
+        double q[CH];
+        bool ok[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            ok[c] = k0 + c * T < m;
+            q[c] = ok[c] ? __ldg(a.kc_grid + k0 + c * T) : 0.0;
+        }
+        int ja[CH];
+        Frac fr[CH];
+        interp_brackets<false, CH>(xa, m, lo_v, hi_v, inv_span, q, ok, ja, fr);
+#pragma unroll
+        for (int c = 0; c < CH; ++c)
+            if (ok[c]) pk[k0 + c * T] = ja[c] >= 0 ? pack_br(0, ja[c], fr[c].f) : pack_br(1, q[c] < lo_v ? 0 : m - 2, 0.f);
     }
     // adjoint of the cross FFT
     const float2 *row = a.zadj_t + (size_t)j * N;

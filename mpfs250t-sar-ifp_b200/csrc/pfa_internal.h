@@ -109,7 +109,10 @@ pfa_status run_host_frames(pfa_plan *p, const void *const *ins, void *const *out
                            size_t out_bytes, FrameFn form, int32_t arg);
 
 // Host-side table builders used when the caller passes NULL for a table (libm based).
-void build_sinc_table(int16_t *tab);   // returns false-free: table from the exact-rational recipe
+void build_sinc_table(int16_t *tab);   // table from the exact-rational recipe, [phase][tap]
+// True when every phase of a [phase][tap] Q15 table has sum |tap| <= 65535 over taps 0-15 and over
+// taps 16-31: the condition for the fixed-point sinc's int32 half-sum accumulation to be exact.
+bool sinc_table_fits_int32(const int16_t *tab);
 void build_twiddles_q15(int G, int16_t *tw2);   // [G/2][2]
 void build_hamming_q15(int len, int size, int32_t *out);
 

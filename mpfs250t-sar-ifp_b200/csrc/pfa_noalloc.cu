@@ -162,6 +162,7 @@ extern "C" pfa_status pfa_form_fixed_noalloc(const pfa_config *cfg, const pfa_fi
 
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const int16_t *sinc = job->sinc_q15 ? job->sinc_q15 : pfa::builtin_sinc_table();
+    if (!pfa::sinc_table_fits_int32(sinc)) return PFA_ERR_BAD_ARG;
     struct Cp { void *dst; const void *src; size_t bytes; } cps[] = {
         {d.f0, job->f0, 4u * m}, {d.df, job->df, 4u * m}, {pr, job->pr, 4u * m}, {d.tan_s, job->tan_s, 4u * m},
         {inv, job->inv_order, 4u * m}, {d.krp, job->kr_grid, 4u * G}, {d.kcp, job->kc_grid, 4u * G},

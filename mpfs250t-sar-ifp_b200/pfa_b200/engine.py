@@ -115,10 +115,11 @@ class FixedPlan(_Plan):
         keep = dict(f0=job["f0"], df=job["df"], pr=job["pr"], tan_s=job["tan_s"], inv_order=inv_order,
                     kr=job["krp"], kc=job["kcp"], hr=np.ascontiguousarray(job["hamr"], np.int32),
                     hc=np.ascontiguousarray(job["hamc"], np.int32),
-                    tw=np.ascontiguousarray(job["twiddle"], np.int16))
+                    tw=np.ascontiguousarray(job["twiddle"], np.int16),
+                    sinc=None if job.get("sinc_q15") is None else np.ascontiguousarray(job["sinc_q15"], np.int16))
         fj = _lib.FixedJob(_ptr(keep["f0"]), _ptr(keep["df"]), _ptr(keep["pr"]), _ptr(keep["tan_s"]),
                            _ptr(keep["inv_order"]), _ptr(keep["kr"]), _ptr(keep["kc"]), _ptr(keep["hr"]),
-                           _ptr(keep["hc"]), _ptr(keep["tw"]), None)
+                           _ptr(keep["hc"]), _ptr(keep["tw"]), _ptr(keep["sinc"]))
         _lib.check(self._lib.pfa_set_fixed_job(self._h, C.byref(fj)), self._h)
         self._job = keep
 

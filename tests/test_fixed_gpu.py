@@ -167,3 +167,21 @@ def test_errors_are_status_codes(torch_cuda):
         img = torch.empty((128, 128), dtype=torch.uint16, device="cuda")
         st = plan._lib.pfa_form_fixed(plan.handle, flat.data_ptr() + 4, img.data_ptr(), None)
         assert st == _lib.BAD_ARG
+
+
+def test_caller_sinc_table(torch_cuda):
+    """A caller-supplied Q15 table: the reference's own table gives the same image; a table whose taps
+    could overflow the int32 half sums (sum |tap| > 65535 over 16 taps) is refused."""
+    from pfa_b200 import tables
+    sc = synth.make_scene(128, 120, n_targets=4, seed=40)
+    tb = geometry.prepare_tables_from_scene(sc)
+    job = geometry.fixed_job(tb, 128)
+    ref, _ = fe.form_image(sc.signal, tb, 128, True, True)
+    with engine.FixedPlan(128, 120, 128, True, True) as plan:
+        job["sinc_q15"] = np.asarray(tables.sinc_table_q15(), np.int16).reshape(256, 32)
+        plan.set_job(job)
+        assert np.array_equal(plan.form(sc.signal), ref)
+        job["sinc_q15"] = np.full((256, 32), 32767, np.int16)
+        with pytest.raises(_lib.PfaError) as ei:
+            plan.set_job(job)
+        assert ei.value.status == _lib.BAD_ARG
