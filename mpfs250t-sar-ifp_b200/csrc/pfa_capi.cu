@@ -167,7 +167,7 @@ pfa_status pfa_plan_create(const pfa_config *cfg, pfa_plan **out) {
         p->fx.range_sinc = c.range_interp == PFA_INTERP_SINC;
         p->fx.az_sinc = c.az_interp == PFA_INTERP_SINC;
         p->ws_bytes = pfa::fixed_workspace_bytes(c.m, c.n, c.grid);
-    } else if (c.mode == PFA_MODE_FLOAT32) {
+    } else if (c.mode == PFA_MODE_FLOAT32 || c.mode == PFA_MODE_MIXED) {
         e = pfa::float_alloc(p->fl, c.m, c.n);
         p->fl.range_sinc = c.range_interp == PFA_INTERP_SINC;
         p->fl.az_sinc = c.az_interp == PFA_INTERP_SINC;
@@ -181,6 +181,10 @@ pfa_status pfa_plan_create(const pfa_config *cfg, pfa_plan **out) {
         p->fl.ept_range = c.fft_ept_range == 8 ? 8 : 16;
         p->ws_bytes = pfa::float_workspace_bytes(c.m, c.n);
         if (e == cudaErrorInvalidValue) { pfa::float_free(p->fl); delete p; return PFA_ERR_BAD_CONFIG; }
+        if (e == cudaSuccess && c.mode == PFA_MODE_MIXED) {
+            p->fl.mixed = 1;
+            e = pfa::mixed_prepare(p->fl);
+        }
     } else {
         delete p;
         return PFA_ERR_BAD_CONFIG;

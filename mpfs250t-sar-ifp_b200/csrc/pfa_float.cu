@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "fft_f32.cuh"
+#include "interp_f32.cuh"
 #include "pfa_internal.h"
 
 namespace pfa {
@@ -32,143 +33,6 @@ constexpr double kC = 299792458.0;
 // FFT: register Stockham radix-16 (fft_f32.cuh).
 template <int L, int E>
 using F32Fft = StockhamFft<L, E>;
-
-// ------------------------------------------------------------------------------------------ async copies
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// ------------------------------------------------------------------------------------------ brackets
-// np.interp bracket on an ascending accessor xa(0..n-1): returns j with xa(j) <= x < xa(j+1) and the
-// fraction, or -1 when x is outside [xa(0), xa(n-1)]; x == xa(n-1) gives j = n-2, frac = 1.
-struct Frac {
-    float f;     // fraction toward the upper natural-order sample (lerp weight)
-    int ph;      // sinc phase round(frac * 32768) >> 7, taken from the float64 ascending fraction
-    int rev;     // descending source axis: taps run in reverse natural order
-};
-
-// phase of the float sinc from a float64 fraction (same rounding as the oracle's np.round)
-__device__ __forceinline__ int sinc_phase(double fd) {
-    return (int)fmin(fmax(rint(fd * 32768.0), 0.0), 32767.0) >> 7;
-}
-
-// Fraction of x in [a, b].  EXACT: float64 fraction (the sinc phase depends on it); else a float32 division.
-template <bool EXACT>
-__device__ __forceinline__ void make_frac(double x, double a, double b, Frac &frac) {
-    if (EXACT) {
-        const double fd = __ddiv_rn(__dsub_rn(x, a), __dsub_rn(b, a));
-        frac.f = (float)fd;
-        frac.ph = sinc_phase(fd);
-    } else {
-        frac.f = __fdiv_rn((float)(x - a), (float)(b - a));
-        frac.ph = 0;
-    }
-    frac.rev = 0;
-}
-
-// Walks from the guess carrying both end values (two loads when the guess is right); bisection after a
-// few steps.
-template <bool EXACT, class F>
-__device__ __forceinline__ int interp_bracket(const F &xa, int n, double x0, double x1, double x, int guess, Frac &frac) {
-    if (!(x >= x0) || !(x <= x1)) return -1;
-    // largest j in [0, n-2] with xa(j) <= x  (xa(0) = x0 <= x <= x1 = xa(n-1))
-    int j = min(max(guess, 0), n - 2);
-    double a = xa(j), b = xa(j + 1);
-    int steps = 0;
-    while (b <= x && j < n - 2) {
-        if (++steps > 8) {
-            int lo = j + 1, hi = n - 2;      // xa(j+1) <= x
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (xa(mid) <= x) lo = mid; else hi = mid - 1;
-            }
-            j = lo;
-            a = xa(j);
-            b = xa(j + 1);
-            break;
-        }
-        ++j;
-        a = b;
-        b = xa(j + 1);
-    }
-    while (a > x && j > 0) {
-        if (++steps > 16) {
-            int lo = 0, hi = j - 1;          // xa(0) <= x < xa(j)
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (xa(mid) <= x) lo = mid; else hi = mid - 1;
-            }
-            j = lo;
-            a = xa(j);
-            b = xa(j + 1);
-            break;
-        }
-        --j;
-        b = a;
-        a = xa(j);
-    }
-    make_frac<EXACT>(x, a, b, frac);
-    return j;
-}
-
-// The same bracket for CH queries at once: every guess and both its end values are loaded before any is
-// tested, so the loads of the CH queries overlap; a query whose guess misses walks from it.
-template <bool EXACT, int CH, class F>
-__device__ __forceinline__ void interp_brackets(const F &xa, int n, double x0, double x1, double inv_span,
-                                                const double (&x)[CH], const bool (&valid)[CH], int (&j)[CH],
-                                                Frac (&frac)[CH]) {
-    int g[CH];
-    double a[CH], b[CH];
-#pragma unroll
-    for (int c = 0; c < CH; ++c) {
-        g[c] = (valid[c] && isfinite(inv_span)) ? min(max((int)((x[c] - x0) * inv_span), 0), n - 2) : 0;
-        a[c] = xa(g[c]);
-        b[c] = xa(g[c] + 1);
-    }
-#pragma unroll
-    for (int c = 0; c < CH; ++c) {
-        j[c] = -1;
-        frac[c] = Frac{0.f, 0, 0};
-        if (!valid[c] || !(x[c] >= x0) || !(x[c] <= x1)) continue;
-        if (a[c] <= x[c] && (x[c] < b[c] || g[c] == n - 2)) {
-            j[c] = g[c];
-            make_frac<EXACT>(x[c], a[c], b[c], frac[c]);
-        } else {
-            j[c] = interp_bracket<EXACT>(xa, n, x0, x1, x[c], g[c], frac[c]);
-        }
-    }
-}
-
-// the same bracket seen from the descending side: lower natural index n-2-j, weights mirrored
-__device__ __forceinline__ void mirror_frac(Frac &fr) {
-    fr.f = 1.0f - fr.f;
-    fr.rev = 1;
-}
-
-// lerp or float sinc of complex64 samples `src` (indexed from `base`) at bracket (j, frac)
-template <bool SINC>
-__device__ __forceinline__ float2 gather_f32(const float2 *src, int base, int sn, int j, Frac fr,
-                                             const float *tab) {
-    if (j < 0) return make_float2(0.f, 0.f);
-    const float frac = fr.f;
-    if (SINC && j >= 15 && j <= sn - 17) {
-        const float *c = tab + fr.ph;                    // table stored [tap][phase]: phases spread over banks
-        const float2 *x = src + (j - 15 - base);
-        float ar = 0.f, ai = 0.f;
-#pragma unroll
-        for (int t = 0; t < 32; ++t) {
-            const float ct = fr.rev ? c[(31 - t) * 256] : c[t * 256];
-            ar = fmaf(ct, x[t].x, ar);
-            ai = fmaf(ct, x[t].y, ai);
-        }
-        return make_float2(ar, ai);
-    }
-    const float2 a = src[j - base], b = src[j + 1 - base];
-    return make_float2(fmaf(frac, b.x - a.x, a.x), fmaf(frac, b.y - a.y, a.y));
-}
 
 // ------------------------------------------------------------------------------------------ K1f
 constexpr int F1_SLOTS = 32, F1_BINS = 128, F1_WARPS = 8, F1_WMAX = 384;
@@ -789,6 +653,7 @@ void float_free(FloatDev &d) {
     dfr(d.f0); dfr(d.df); dfr(d.flast); dfr(d.pr); dfr(d.tan_s); dfr(d.order); dfr(d.kr); dfr(d.kc); dfr(d.ham_m64);
     dfr(d.ham_n64); dfr(d.twm); dfr(d.twn); dfr(d.tabf); dfr(d.p1); dfr(d.y1);
     dfr(d.af_zadj); dfr(d.af_acc); dfr(d.af_dacc);
+    mixed_free(d);
 }
 
 cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int detect, cudaStream_t st, StageProf *prof) {
@@ -810,11 +675,14 @@ cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int dete
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = pf.mark(st, "pass1")) != cudaSuccess) return e;
-    e = d.az_sinc ? dispatch_pass2<true>(d, st) : dispatch_pass2<false>(d, st);
+    // mixed mode: tensor-core FFTs on the axes whose lines are 2048..8192 points, FP32 FFTs elsewhere
+    if (d.mixed && mixed_axis(d.Lm)) e = mixed_pass2(d, st);
+    else e = d.az_sinc ? dispatch_pass2<true>(d, st) : dispatch_pass2<false>(d, st);
     if (e != cudaSuccess) return e;
     if ((e = pf.mark(st, "pass2_win_fft1")) != cudaSuccess) return e;
     const float scale = d.sgn > 0 ? 1.0f / ((float)d.m2 * (float)d.n2) : 1.0f;
-    e = dispatch_fft2(d, out, detect, scale, st);
+    if (d.mixed && mixed_axis(d.Ln)) e = mixed_fft2(d, out, detect, scale, st);
+    else e = dispatch_fft2(d, out, detect, scale, st);
     if (e != cudaSuccess) return e;
     return pf.mark(st, "fft2_detect");
 }
@@ -973,6 +841,8 @@ pfa_status pfa_form_float(pfa_plan *p, const float *sig_dev, void *out_dev, int3
     if (!p->job_ready) return ffail(p, PFA_ERR_NOT_READY, "pfa_set_float_job not called");
     if (detect < PFA_DETECT_MAG || detect > PFA_DETECT_COMPLEX) return ffail(p, PFA_ERR_BAD_ARG, "bad detect mode");
     if (reinterpret_cast<uintptr_t>(sig_dev) & 7) return ffail(p, PFA_ERR_BAD_ARG, "signal must be 8-byte aligned");
+    if (p->fl.mixed && (reinterpret_cast<uintptr_t>(out_dev) & 15))
+        return ffail(p, PFA_ERR_BAD_ARG, "mixed mode: output must be 16-byte aligned");
     DevGuard dg(p->device);
     cudaError_t e = pfa::float_form(p->fl, reinterpret_cast<const float2 *>(sig_dev), out_dev, detect,
                                     reinterpret_cast<cudaStream_t>(stream), &p->prof);

@@ -48,6 +48,13 @@ struct FloatDev {
     float2 *af_zadj = nullptr;         // [n][m2] autofocus: adjoint of the range FFT (range-bin rows)
     double *af_acc = nullptr;          // [2] sum I, sum I log I
     float *af_dacc = nullptr;          // [mpad] per-slot gradient accumulators
+    // split-precision (mixed) mode: tensor-core FFTs for lines of 2048..8192 points
+    int mixed = 0;
+    uint4 *mx_f128 = nullptr;          // F_128 TMEM image [128 lanes][256 columns] of fp16 pairs
+    uint4 *mx_fn2m = nullptr, *mx_fn2n = nullptr;   // F_{m2/128}, F_{n2/128} shared-memory images
+    int *mx_err = nullptr;             // device flag: a tensor-core completion wait timed out
+    int mx_clusters = 0;               // resident 8-CTA clusters of the mixed pass 2
+    int sms = 0;                       // SM count of the plan's device
 };
 
 }  // namespace pfa
@@ -102,6 +109,13 @@ cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int dete
 size_t float_workspace_bytes(int m, int n);
 cudaError_t float_alloc(FloatDev &d, int m, int n);
 void float_free(FloatDev &d);
+
+// Split-precision tensor-core FFT mode (pfa_mixed.cu).
+bool mixed_axis(int L);                                  // 2^L-point lines run on the tensor cores
+cudaError_t mixed_prepare(FloatDev &d);                  // tables, SM/cluster occupancy (plan creation)
+void mixed_free(FloatDev &d);
+cudaError_t mixed_pass2(const FloatDev &d, cudaStream_t st);
+cudaError_t mixed_fft2(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st);
 
 // Pipelined host frames (pfa_capi.cu): form(plan, in_dev, out_dev, stream, arg) runs one frame.
 typedef pfa_status (*FrameFn)(pfa_plan *p, const void *in_dev, void *out_dev, cudaStream_t st, int32_t arg);
