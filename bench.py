@@ -169,8 +169,9 @@ def _device_ms(fn, steps, warmup):
 
 def measure_modes(a, local):
     """The other configurations of the metric, device-timed at N=1: the NDSU-shaped float frame
-    (8167x8192 -> 8192^2; FP32 lerp as form_image_pfa, FP32 32-tap sinc) and the image-entropy autofocus
-    gradient on the 4096^2 scene (grads/s)."""
+    (8167x8192 -> 8192^2; FP32 lerp as form_image_pfa, FP32 32-tap sinc, and both in the split-precision
+    tensor-core FFT mode with its error against the FP32 image), the image-entropy autofocus gradient on
+    the 4096^2 scene (grads/s) and the 16-scene batch."""
     import numpy as np
     import torch
     from pfa_b200 import autofocus, engine, geometry, synth
@@ -179,8 +180,10 @@ def measure_modes(a, local):
     out = {}
     sc, sig = synth.make_scene_device(8167, 8192, device=f"cuda:{local}", **{k: v for k, v in synth.WORKLOADS["ndsu_8167x8192"].items() if k not in ("m", "n")})
     tables = geometry.prepare_tables_from_scene(sc)
-    for name, rs in (("float_fp32_lerp", False), ("float_fp32_sinc", True)):
-        with engine.FloatPlan(8167, 8192, rs, rs, device=local) as plan:
+    ref_c = {}
+    for name, rs, mixed in (("float_fp32_lerp", False, False), ("float_fp32_sinc", True, False),
+                            ("float_mixed_lerp", False, True), ("float_mixed_sinc", True, True)):
+        with engine.FloatPlan(8167, 8192, rs, rs, mixed=mixed, device=local) as plan:
             plan.set_tables(tables)
             img = torch.empty((8192, 8192), dtype=torch.float32, device=sig.device)
             ms = _device_ms(lambda: plan.form(sig, out=img), steps, 3)
@@ -188,10 +191,20 @@ def measure_modes(a, local):
             plan.form(sig, out=img)
             st = plan.stage_times()
             plan.set_profiling(False)
+            cz = plan.form(sig, detect="complex")
         fb = sum(stage_bytes(s, 8167, 8192, 8192, "float") for s in st)
         out[name] = {"workload": "ndsu_8167x8192 -> 8192^2", "ms_per_frame": round(ms, 4),
                      "stages_ms": {k: round(v, 4) for k, v in st.items()},
                      "frame_bytes": fb, "frame_frac_of_hbm": round(fb / (ms * 1e-3) / 1e9 / _peaks()[0], 4)}
+        if not mixed:
+            ref_c[rs] = (cz, ms)
+        else:
+            # the FP32 image is pinned to FP64 at <= 1e-6 (tests); the mixed error budget is 1e-4
+            r, ms32 = ref_c[rs]
+            out[name]["rel_l2_vs_fp32_complex"] = float(torch.linalg.vector_norm(cz - r) / torch.linalg.vector_norm(r))
+            out[name]["speed_vs_fp32"] = round(ms32 / ms, 3)
+        del cz
+    ref_c.clear()
     del sig
     wl = synth.WORKLOADS["autofocus_4096"]
     sc, sig = synth.make_scene_device(4096, 4096, device=f"cuda:{local}", **{k: v for k, v in wl.items() if k not in ("m", "n")})
