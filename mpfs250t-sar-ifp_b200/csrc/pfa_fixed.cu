@@ -37,6 +37,14 @@ __device__ __forceinline__ int lo16(uint32_t p) { return (int)(int16_t)(p & 0xff
 __device__ __forceinline__ int hi16(uint32_t p) { return (int)(int16_t)(p >> 16); }
 __device__ __forceinline__ int wrap16(int v) { return (int)(int16_t)(v & 0xffff); }
 
+// 16-byte global -> shared copies that complete asynchronously (both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // Smallest e with M <= 32767 * 2^e, i.e. ceil(log2(M / 32767)) of fixedpoint.fit_scale for a float32
 // maximum M (exact: M/32767 is either an exact power of two or at least 2^-24 away from one).
 __device__ __forceinline__ int q0_exponent(uint32_t bits) {
@@ -438,11 +446,12 @@ __global__ void __launch_bounds__((1 << L) / E) k_fx_pass2_fft(Pass2Args a) {
     using F = BfpFft<L, E>;
     constexpr int N = F::N, T = F::T;
     extern __shared__ __align__(16) unsigned char smem[];
-    // layout: [region A: src coords f32[m] + row u32[m] | exchange buffer] [tw N-1] [sinc] [red]
+    // layout: [region A: row u32[m] + src coords f32[m] | exchange buffer] [tw N] [sinc] [red]
     const int m = a.m;
-    const size_t regA = max((size_t)8 * m, (size_t)4 * (N + N / 32));
-    float *srcx = reinterpret_cast<float *>(smem);
-    uint32_t *row = reinterpret_cast<uint32_t *>(smem + 4 * (size_t)m);
+    const size_t rowb = ((size_t)4 * m + 15) & ~(size_t)15;
+    const size_t regA = (max(rowb + (size_t)4 * m, (size_t)4 * (N + N / 32)) + 15) & ~(size_t)15;
+    uint32_t *row = reinterpret_cast<uint32_t *>(smem);
+    float *srcx = reinterpret_cast<float *>(smem + rowb);
     uint32_t *xbuf = reinterpret_cast<uint32_t *>(smem);
     uint32_t *tw = reinterpret_cast<uint32_t *>(smem + regA);
     int16_t *tab = reinterpret_cast<int16_t *>(smem + regA + 4 * (size_t)N);
@@ -450,17 +459,18 @@ __global__ void __launch_bounds__((1 << L) / E) k_fx_pass2_fft(Pass2Args a) {
 
     const int tid = threadIdx.x;
     const int j = blockIdx.x;                       // range bin (< n)
+    // the p1 row, the twiddles and the sinc table stream in while the source coordinates are computed
+    {
+        const uint32_t *src = a.p1 + (size_t)j * a.mpad;            // 128-byte aligned rows, mpad >= m
+        for (int c = tid; c < (m + 3) >> 2; c += T) cp_async16(row + 4 * c, src + 4 * c);
+        for (int c = tid; c < N / 4; c += T) cp_async16(tw + 4 * c, a.tw + 4 * c);
+        if (SINC)
+            for (int c = tid; c < 256 * kSincTaps / 8; c += T) cp_async16(tab + 8 * c, a.sinc + 8 * c);
+        cp_async_commit();
+    }
     const float krj = a.krp[j];
-    for (int r = tid; r < m; r += T) {
-        srcx[r] = __fmul_rn(krj, a.tan_s[r]);      // KRp[j] * tan_s in float32 (silicon_emulator.py:152)
-        row[r] = a.p1[(size_t)j * a.mpad + r];
-    }
-    for (int i = tid; i < N - 1; i += T) tw[i] = a.tw[i];
-    if (SINC) {
-        const uint32_t *s = reinterpret_cast<const uint32_t *>(a.sinc);
-        uint32_t *d = reinterpret_cast<uint32_t *>(tab);
-        for (int i = tid; i < 256 * kSincTaps / 2; i += T) d[i] = s[i];
-    }
+    for (int r = tid; r < m; r += T) srcx[r] = __fmul_rn(krj, a.tan_s[r]);   // KRp[j] * tan_s in float32 (silicon_emulator.py:152)
+    cp_async_wait_all();
     __syncthreads();
 
     const bool asc = srcx[m - 1] >= srcx[0];
@@ -515,12 +525,14 @@ __global__ void __launch_bounds__((1 << L) / E) k_fx_fft2(Fft2Args a) {
     using F = BfpFft<L, E>;
     constexpr int N = F::N, T = F::T;
     extern __shared__ __align__(16) unsigned char smem[];
+    constexpr size_t XB = ((size_t)4 * (N + N / 32) + 15) & ~(size_t)15;   // exchange buffer, 16-byte multiple
     uint32_t *xbuf = reinterpret_cast<uint32_t *>(smem);
-    uint32_t *tw = reinterpret_cast<uint32_t *>(smem + 4 * (size_t)(N + N / 32));
-    int(*red)[32] = reinterpret_cast<int(*)[32]>(smem + 4 * (size_t)(N + N / 32) + 4 * (size_t)N);
+    uint32_t *tw = reinterpret_cast<uint32_t *>(smem + XB);
+    int(*red)[32] = reinterpret_cast<int(*)[32]>(smem + XB + 4 * (size_t)N);
     const int tid = threadIdx.x;
     const int k = blockIdx.x;                       // cross bin
-    for (int i = tid; i < N - 1; i += T) tw[i] = a.tw[i];
+    for (int c = tid; c < N / 4; c += T) cp_async16(tw + 4 * c, a.tw + 4 * c);
+    cp_async_commit();
     const int emax1 = a.ctrl[1];
     int xr[E], xi[E];
 #pragma unroll
@@ -537,6 +549,7 @@ __global__ void __launch_bounds__((1 << L) / E) k_fx_fft2(Fft2Args a) {
         xr[vv] = r;
         xi[vv] = i;
     }
+    cp_async_wait_all();
     __syncthreads();
     const int e_row = F::run(xr, xi, xbuf, tw, red, tid);
     uint32_t *out = a.y2 + (size_t)k * N;
@@ -556,16 +569,24 @@ __global__ void __launch_bounds__(256) k_fx_detect(const uint32_t *__restrict__ 
     const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
     const int emax2 = ctrl[2];
     const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;   // 64 x 4
-    for (int kk = ty; kk < 64; kk += 4) {
-        const int k = k0 + kk;
-        const uint32_t v = __ldcs(y2 + (size_t)k * G + j0 + tx);
-        const int s = min(emax2 - e2[k], 31);
-        const int r = sat16(lo16(v) >> s), i = sat16(hi16(v) >> s);
+    // all 16 loads of this thread in flight before any arithmetic
+    uint32_t v[16];
+    int s[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int k = k0 + ty + 4 * u;
+        v[u] = __ldcs(y2 + (size_t)k * G + j0 + tx);
+        s[u] = __ldg(e2 + k);
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int sh = min(emax2 - s[u], 31);
+        const int r = lo16(v[u]) >> sh, i = hi16(v[u]) >> sh;     // an arithmetic shift keeps int16 range
         const unsigned p = (unsigned)(r * r) + (unsigned)(i * i);
         unsigned q = (unsigned)sqrtf((float)p);
         while (q * q > p) --q;
         while ((q + 1) * (q + 1) <= p) ++q;
-        t[tx][kk] = (uint16_t)min(q, 65535u);
+        t[tx][ty + 4 * u] = (uint16_t)min(q, 65535u);
     }
     __syncthreads();
     for (int jj = ty; jj < 64; jj += 4) img[(size_t)(j0 + jj) * G + k0 + tx] = t[jj][tx];
@@ -579,12 +600,14 @@ struct FixedLaunch {
     static constexpr int T = N / E;
 
     static size_t pass2_smem(int m, bool sinc) {
-        size_t regA = (size_t)8 * m;
-        size_t xb = (size_t)4 * (N + N / 32);
+        const size_t rowb = ((size_t)4 * m + 15) & ~(size_t)15;
+        size_t regA = rowb + (size_t)4 * m;
+        const size_t xb = (size_t)4 * (N + N / 32);
         if (xb > regA) regA = xb;
+        regA = (regA + 15) & ~(size_t)15;
         return regA + 4 * (size_t)N + (sinc ? 2 * 256 * kSincTaps : 0) + 2 * 32 * 4;
     }
-    static size_t fft2_smem() { return 4 * (size_t)(N + N / 32) + 4 * (size_t)N + 2 * 32 * 4; }
+    static size_t fft2_smem() { return (((size_t)4 * (N + N / 32) + 15) & ~(size_t)15) + 4 * (size_t)N + 2 * 32 * 4; }
 
     static cudaError_t run(const FixedDev &d, const float *sig, const uint32_t *sig_iq, uint16_t *img,
                            cudaStream_t st, StageProf &pf) {
