@@ -4,7 +4,7 @@
 // Kernels (one stream, stream-ordered):
 //   k_q0max        block max of |re|,|im| over the complex64 signal (fixedpoint.fit_scale, :19-26)
 //   k_fx_pass1     Q0 quantise + pass-1 bracket search (FP64) + 32-tap sinc / 2-tap lerp gather per
-//                  pulse; a 32-slot x 256-bin shared tile turns the pulse-major output into range-bin
+//                  pulse; a 32-slot x 128-bin shared tile turns the pulse-major output into range-bin
 //                  rows (corner turn #1, silicon_emulator.py:142-148)
 //   k_fx_pass2_fft pass-2 bracket search + gather + Q15 window + 13-stage per-row BFP FFT along the
 //                  cross axis (silicon_emulator.py:150-156, 165-195, 198-205 with fixedpoint.py:266-289)
@@ -184,9 +184,9 @@ __global__ void k_q0exp(int32_t *ctrl) { ctrl[3] = q0_exponent((uint32_t)ctrl[0]
 
 // ------------------------------------------------------------------------------------------ K1
 constexpr int P1_SLOTS = 32;          // sorted pulse slots per CTA
-constexpr int P1_BINS = 256;          // range bins per CTA
+constexpr int P1_BINS = 128;          // range bins per CTA
 constexpr int P1_WARPS = 8;
-constexpr int P1_WMAX = 512;          // per-warp source window (samples)
+constexpr int P1_WMAX = 384;          // per-warp source window (samples)
 
 struct Pass1Args {
     const float2 *sig;                // complex64 input (or nullptr)
@@ -204,7 +204,7 @@ constexpr size_t P1_SMEM_WIN = (size_t)P1_WARPS * P1_WMAX * 4;
 constexpr size_t p1_smem(bool sinc) { return P1_SMEM_TILE + P1_SMEM_WIN + (sinc ? 2 * 256 * kSincTaps : 0); }
 
 template <bool SINC>
-__global__ void __launch_bounds__(256) k_fx_pass1(Pass1Args a) {
+__global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t(*tile)[P1_SLOTS + 1] = reinterpret_cast<uint32_t(*)[P1_SLOTS + 1]>(smem);
     uint32_t(*win)[P1_WMAX] = reinterpret_cast<uint32_t(*)[P1_WMAX]>(smem + P1_SMEM_TILE);
