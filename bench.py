@@ -120,18 +120,23 @@ def _dist():
     return ws, rank, local
 
 
-def _traffic(kernel: str, workload: str):
-    """DRAM bytes per launch from the committed ncu summary (profiles/<kernel>__<workload>.md)."""
+def _profile_value(kernel: str, workload: str, key: str):
+    """A `key: value` line of the committed ncu summary profiles/<kernel>__<workload>.md (or None)."""
     p = ROOT / "profiles" / f"{kernel}__{workload}.md"
     if not p.is_file():
         return None
     for ln in p.read_text().splitlines():
-        if ln.startswith("dram_bytes_per_launch:"):
+        if ln.startswith(key + ":"):
             try:
                 return float(ln.split(":", 1)[1].split()[0])
             except ValueError:
                 return None
     return None
+
+
+def _traffic(kernel: str, workload: str):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the ncu summary."""
+    return _profile_value(kernel, workload, "dram_bytes_per_launch")
 
 
 def stage_bytes(stage: str, m: int, n: int, G: int, mode: str = "fixed") -> float:
@@ -390,7 +395,11 @@ def run_ours(a, ws, rank, local):
                      "unit": "GB/s", "frac": round(ach / hbm, 4), "peak_kind": f"of {peak_kind}",
                      "traffic": traffic, "algorithmic_bytes": stage_bytes(top, m, n, G, mode),
                      "frame_bytes": frame_bytes,
-                     "frame_frac": round(frame_bytes / (ms_per_frame * 1e-3) / 1e9 / hbm, 4)},
+                     "frame_frac": round(frame_bytes / (ms_per_frame * 1e-3) / 1e9 / hbm, 4),
+                     # what bounds it instead: pipe utilisation of the same kernel from the ncu summary
+                     "compute": {"pipe": "integer ALU" if mode == "fixed" else "FP32/LSU",
+                                 "alu_pipe_active_pct": _profile_value(kname, a.workload, "alu_pipe_active_pct"),
+                                 "issue_active_pct": _profile_value(kname, a.workload, "issue_active_pct")}},
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms/frame", "h2d_bytes_per_step": int(sc.signal.nbytes),
                 "d2h_bytes_per_step": int(out_bytes), "frames": ne2e, "api": "pfa_form_*_host_frames (pipelined)",
                 "single_frame_ms": round(e2e_single_ms, 4)},

@@ -406,8 +406,17 @@ struct BfpFft {
                 if (lane == 0) red[rbuf][warp] = (int)mx;
                 __syncthreads();
                 int rowmax = 0;
+                if constexpr (WARPS % 4 == 0) {
+                    const int4 *r4 = reinterpret_cast<const int4 *>(red[rbuf]);   // 128-byte rows, 16-byte aligned
 #pragma unroll
-                for (int q = 0; q < WARPS; ++q) rowmax = max(rowmax, red[rbuf][q]);
+                    for (int q = 0; q < WARPS / 4; ++q) {
+                        const int4 v4 = r4[q];
+                        rowmax = max(rowmax, max(max(v4.x, v4.y), max(v4.z, v4.w)));
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < WARPS; ++q) rowmax = max(rowmax, red[rbuf][q]);
+                }
                 rbuf ^= 1;
                 // max(0, ceil(log2((mx + 1) / 32767))) on integers
                 int sh = 0;
@@ -541,9 +550,9 @@ __global__ void __launch_bounds__((1 << L) / E) k_fx_fft2(Fft2Args a) {
         int r = 0, i = 0;
         if (jr < a.n) {
             const uint32_t v = __ldg(a.y1 + (size_t)jr * N + k);
-            const int s = min(emax1 - __ldg(a.e1 + jr), 31);
-            r = sat16(lo16(v) >> s);
-            i = sat16(hi16(v) >> s);
+            const int s = min(emax1 - __ldg(a.e1 + jr), 31);   // >= 0: the shifted int16 stays in range
+            r = lo16(v) >> s;
+            i = hi16(v) >> s;
         }
         const int vv = (int)(__brev((unsigned)u) >> (32 - F::LE));
         xr[vv] = r;
