@@ -73,6 +73,96 @@ def prepare_tables(reader, meta, deci_pulse=1, deci_sample=1, crop_sample=0):
             "dims": (m, n), "deci": (mu, nu), "n_vec": n_vec, "n_samp": n_samp, "samp0": samp0}
 
 
+class AffineFreq:
+    """The (m, n) RF frequency table of prepare_tables, freq[i, k] = sc0_i + k * step_i (k = k0 + column),
+    without materialising it: columns and rows are computed on demand with the same float64 operations
+    as the NumPy broadcast (so every element is bit-identical), ``np.asarray`` builds the full array."""
+
+    def __init__(self, sc0: np.ndarray, step: np.ndarray, k0: int, n: int):
+        self.sc0 = np.asarray(sc0, np.float64)
+        self.step = np.asarray(step, np.float64)
+        self.k0, self.n = int(k0), int(n)
+        self.shape = (len(self.sc0), self.n)
+        self.ndim, self.dtype = 2, np.dtype(np.float64)
+
+    def column(self, c: int) -> np.ndarray:
+        c = c + self.n if c < 0 else c
+        return self.sc0 + np.float64(self.k0 + c) * self.step
+
+    def __getitem__(self, idx):
+        if isinstance(idx, tuple) and len(idx) == 2 and idx[0] == slice(None) and isinstance(idx[1], (int, np.integer)):
+            return self.column(int(idx[1]))
+        return np.asarray(self)[idx]
+
+    def __array__(self, dtype=None, copy=None):
+        k = self.k0 + np.arange(self.n)
+        a = self.sc0[:, None] + k[None, :] * self.step[:, None]
+        return a if dtype is None else a.astype(dtype)
+
+
+def prepare_tables_fast(reader, meta, deci_pulse=1, deci_sample=1, crop_sample=0):
+    """prepare_tables in O(m + n) with bit-identical outputs (mpfs/host/sar_pipeline.py:36-115).
+
+    The reference materialises (m, n) float64 arrays (freq, 2 freq / c, kr, KR x tan(phi)) only to take
+    row extremes and a global max.  Every one of them is monotone: fl(k * step) and fl(sc0 + x) are
+    monotone in k, so are fl(2 f / c) and fl(kmag * pr), hence each pulse's kr extremes are its end
+    samples; and fl(|a| |b|) is monotone in both factors, hence max |KR x tan(phi)| is the rounded product
+    of the two largest magnitudes.  ``freq`` is returned as an ``AffineFreq`` view; the (m, n) float32
+    window of the reference is not built (the engine applies the two Hamming tapers on the fly).
+    """
+    mu, nu = max(1, deci_pulse), max(1, deci_sample)
+    n_vec, n_samp = reader.get_data_size_as_tuple()[0]
+    sgn = int(meta.Global.SGN)
+    tx = reader.read_pvp_variable("TxPos", 0)[::mu]
+    rcv = reader.read_pvp_variable("RcvPos", 0)[::mu]
+    srp = reader.read_pvp_variable("SRPPos", 0)[::mu]
+    sc0 = reader.read_pvp_variable("SC0", 0)[::mu]
+    scss = reader.read_pvp_variable("SCSS", 0)[::mu]
+    apc = 0.5 * (tx + rcv)
+    plan = meta.SceneCoordinates.ReferenceSurface.Planar
+    uiax = np.array([plan.uIAX.X, plan.uIAX.Y, plan.uIAX.Z])
+    uiay = np.array([plan.uIAY.X, plan.uIAY.Y, plan.uIAY.Z])
+    los = srp - apc
+    u = los / np.linalg.norm(los, axis=1, keepdims=True)
+    ax = u @ uiax
+    ay = u @ uiay
+    m = len(range(0, n_vec, mu))
+    n = len(range(0, n_samp, nu))
+    d0 = 0
+    if crop_sample and crop_sample < n:
+        d0 = (n - crop_sample) // 2
+        n = crop_sample
+    samp0 = d0 * nu
+    freq = AffineFreq(sc0, scss * nu, d0, n)
+    dx, dy = ax.mean(), ay.mean()
+    dn = np.hypot(dx, dy)
+    dx, dy = dx / dn, dy / dn
+    cx, cy = -dy, dx
+    pr = ax * dx + ay * dy
+    pc = ax * cx + ay * cy
+    tan_phi = pc / pr
+    ka = (2.0 * freq.column(0) / C_LIGHT) * pr
+    kb = (2.0 * freq.column(n - 1) / C_LIGHT) * pr
+    rmax, rmin = np.maximum(ka, kb), np.minimum(ka, kb)
+    kr_lo, kr_hi = rmax.min(), rmin.max()
+    if kr_lo > kr_hi:
+        kr_lo, kr_hi = rmin.min(), rmax.max()
+    KR = np.linspace(kr_lo, kr_hi, n)
+    kc_max = np.abs(KR[np.argmax(np.abs(KR))] * tan_phi[np.argmax(np.abs(tan_phi))])
+    KC = np.linspace(-kc_max, kc_max, m)
+    geo = {"dc": 1.0 / (KC[-1] - KC[0]), "dr": 1.0 / (KR[-1] - KR[0]),
+           "dhat": (dx, dy), "chat": (cx, cy)}
+    return {"ax": ax, "ay": ay, "freq": freq, "sgn": sgn, "KR": KR, "KC": KC, "tan_phi": tan_phi,
+            "geo": geo, "center_ecef": srp[0], "uiax": uiax, "uiay": uiay,
+            "dims": (m, n), "deci": (mu, nu), "n_vec": n_vec, "n_samp": n_samp, "samp0": samp0}
+
+
+def prepare_tables_from_scene_fast(scene, deci=1):
+    from .synth import FakeReader
+    rd = FakeReader(scene)
+    return prepare_tables_fast(rd, rd.cphd_meta, deci, deci)
+
+
 def prepare_tables_from_scene(scene, deci=1):
     from .synth import FakeReader
     rd = FakeReader(scene)
