@@ -47,7 +47,16 @@ typedef enum pfa_status {
 } pfa_status;
 
 enum pfa_mode { PFA_MODE_FIXED = 0, PFA_MODE_FLOAT32 = 1, PFA_MODE_MIXED = 2 };
-enum pfa_interp { PFA_INTERP_LERP = 0, PFA_INTERP_SINC = 1 };
+/* Resampler of a pass.  CUBIC (fixed mode only) is the 4-tap Lagrange interpolator of the RTL vector
+ * generator (gen_resample_vectors.gather_cubic, mpfs/fpga/tb/gen_resample_vectors.py:177-195, 298-325),
+ * offered for A/B comparison with board captures; its edge brackets use the integer 2-tap lerp. */
+enum pfa_interp { PFA_INTERP_LERP = 0, PFA_INTERP_SINC = 1, PFA_INTERP_CUBIC = 2 };
+
+/* Fixed-mode detection order.  EMULATOR: global renorm (>> (emax - e_row), int16) then integer |z|, as
+ * silicon_emulator.form_image (mpfs/host/silicon_emulator.py:247-249).  FUSED: |z| at the row's native
+ * exponent, then the magnitude shifted (model_detect_fusion.order_B_fused, mpfs/host/
+ * model_detect_fusion.py:56-71): the silicon order when detect is fused into the FFT unloader. */
+enum pfa_detect_order { PFA_DETECT_ORDER_EMULATOR = 0, PFA_DETECT_ORDER_FUSED = 1 };
 
 /* Output layout of the float path. */
 enum pfa_layout {
@@ -74,7 +83,8 @@ typedef struct pfa_config {
     int32_t fft_ept_cross; /* float: complex values per thread in the cross FFT (8 or 16; 0 = 16),
                               i.e. CTA size pow2(m)/ept -- the tile shape the autotuner picks   */
     int32_t fft_ept_range; /* float: same for the range FFT (pow2(n)/ept threads)               */
-    int32_t reserved[7];
+    int32_t detect_order;  /* fixed: pfa_detect_order (0 = emulator order)                      */
+    int32_t reserved[6];
 } pfa_config;
 
 /* Fixed-point job: host pointers, copied at pfa_set_fixed_job.  Built exactly as

@@ -149,8 +149,11 @@ pfa_status pfa_plan_create(const pfa_config *cfg, pfa_plan **out) {
     *out = nullptr;
     const pfa_config c = *cfg;
     if (c.m < 2 || c.n < 2) return PFA_ERR_BAD_DIMS;
-    if ((c.range_interp != PFA_INTERP_LERP && c.range_interp != PFA_INTERP_SINC) ||
-        (c.az_interp != PFA_INTERP_LERP && c.az_interp != PFA_INTERP_SINC))
+    auto interp_ok = [&](int v) {
+        return v == PFA_INTERP_LERP || v == PFA_INTERP_SINC || (v == PFA_INTERP_CUBIC && c.mode == PFA_MODE_FIXED);
+    };
+    if (!interp_ok(c.range_interp) || !interp_ok(c.az_interp)) return PFA_ERR_BAD_CONFIG;
+    if (c.detect_order != PFA_DETECT_ORDER_EMULATOR && !(c.detect_order == PFA_DETECT_ORDER_FUSED && c.mode == PFA_MODE_FIXED))
         return PFA_ERR_BAD_CONFIG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= c.device || c.device < 0) return PFA_ERR_NO_DEVICE;
@@ -166,6 +169,9 @@ pfa_status pfa_plan_create(const pfa_config *cfg, pfa_plan **out) {
         e = pfa::fixed_alloc(p->fx, c.m, c.n, c.grid);
         p->fx.range_sinc = c.range_interp == PFA_INTERP_SINC;
         p->fx.az_sinc = c.az_interp == PFA_INTERP_SINC;
+        p->fx.range_cubic = c.range_interp == PFA_INTERP_CUBIC;
+        p->fx.az_cubic = c.az_interp == PFA_INTERP_CUBIC;
+        p->fx.fused_detect = c.detect_order == PFA_DETECT_ORDER_FUSED;
         p->ws_bytes = pfa::fixed_workspace_bytes(c.m, c.n, c.grid);
     } else if (c.mode == PFA_MODE_FLOAT32 || c.mode == PFA_MODE_MIXED) {
         e = pfa::float_alloc(p->fl, c.m, c.n);

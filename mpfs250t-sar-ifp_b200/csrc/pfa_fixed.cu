@@ -166,6 +166,43 @@ __device__ __forceinline__ uint32_t lerp_gather(const uint32_t *win, int base, B
     return pack16(sat16(ar + sr), sat16(ai + si));
 }
 
+// floor(a / b) for b > 0 (C division truncates toward zero)
+__device__ __forceinline__ int floordiv64(long long a, long long b) {
+    const long long q = a / b;
+    return (int)((a % b != 0 && a < 0) ? q - 1 : q);
+}
+
+// 4-point cubic Lagrange taps at mu = w / 2^15 in Q15 (gen_resample_vectors.lagrange_taps_q15,
+// mpfs/fpga/tb/gen_resample_vectors.py:177-195): each tap's exact value x 2^15 is N / D with integer
+// N (|N| < 2^48) and D, rounded half up once: floor((2 N + D) / (2 D)).
+__device__ __forceinline__ void lagrange_q15(int w, int (&c)[4]) {
+    const long long W = w, A = W + 32768, B = W - 32768, C = W - 65536;
+    const long long d6 = 6LL << 30, d2 = 1LL << 31;
+    c[0] = floordiv64(2 * (-(W * B * C)) + d6, 2 * d6);
+    c[1] = floordiv64(2 * (A * B * C) + d2, 2 * d2);
+    c[2] = floordiv64(2 * (-(A * W * C)) + d2, 2 * d2);
+    c[3] = floordiv64(2 * (A * W * B) + d6, 2 * d6);
+}
+
+// gen_resample_vectors.gather_cubic (:298-325): taps at idx-1..idx+2 where 1 <= idx <= sn-3, sum >> 15
+// (floor), sat16; other live brackets take the integer 2-tap lerp; idx < 0 gives 0.
+__device__ __forceinline__ uint32_t cubic_gather(const uint32_t *win, int base, int sn, Bracket b) {
+    if (b.idx < 0) return 0u;
+    if (b.idx >= 1 && b.idx <= sn - 3) {
+        int c[4];
+        lagrange_q15(b.wq, c);
+        const uint32_t *x = win + (b.idx - 1 - base);
+        long long ar = 0, ai = 0;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            ar += (long long)c[t] * lo16(x[t]);
+            ai += (long long)c[t] * hi16(x[t]);
+        }
+        return pack16((int)sat16ll(ar >> 15), (int)sat16ll(ai >> 15));
+    }
+    return lerp_gather<false>(win, base, b);
+}
+
 // ------------------------------------------------------------------------------------------ K0
 __global__ void k_q0max(const float4 *__restrict__ sig4, long long n4, const float *__restrict__ tail,
                         int ntail, uint32_t *__restrict__ out_bits) {
@@ -197,6 +234,7 @@ struct Pass1Args {
     const int32_t *ctrl;
     uint32_t *p1;
     int m, n, mpad;
+    int cubic;                        // 4-tap Lagrange instead of the lerp (SINC off)
 };
 
 constexpr size_t P1_SMEM_TILE = (size_t)P1_BINS * (P1_SLOTS + 1) * 4;
@@ -262,8 +300,8 @@ __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
         hi_i = __reduce_max_sync(0xffffffffu, hi_i);
         int wlo = 0, whi = 0;
         if (hi_i >= 0) {
-            wlo = max(0, lo_i + (SINC ? kSincFirst : 0));
-            whi = min(n, hi_i + (SINC ? kSincTaps + kSincFirst : 2));
+            wlo = max(0, lo_i + (SINC ? kSincFirst : (a.cubic ? -1 : 0)));
+            whi = min(n, hi_i + (SINC ? kSincTaps + kSincFirst : (a.cubic ? 3 : 2)));
         }
         const bool fits = (whi - wlo) <= P1_WMAX;
         uint32_t *w = win[warp];
@@ -287,12 +325,14 @@ __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
             uint32_t out = 0u;
             if (j0 + jj < n && br[t].idx >= 0) {
                 if (fits) {
-                    out = SINC ? sinc_gather(w, wlo, n, br[t], tab) : lerp_gather<true>(w, wlo, br[t]);
+                    out = SINC ? sinc_gather(w, wlo, n, br[t], tab)
+                               : (a.cubic ? cubic_gather(w, wlo, n, br[t]) : lerp_gather<true>(w, wlo, br[t]));
                 } else {
                     // Window wider than the staging buffer: gather straight from global memory.
                     uint32_t tmp[kSincTaps + 1];
-                    const int base = SINC ? max(0, br[t].idx + kSincFirst) : br[t].idx;
-                    const int cnt = SINC ? min(n, br[t].idx + kSincTaps + kSincFirst) - base : 2;
+                    const int base = SINC ? max(0, br[t].idx + kSincFirst) : (a.cubic ? max(0, br[t].idx - 1) : br[t].idx);
+                    const int cnt = SINC ? min(n, br[t].idx + kSincTaps + kSincFirst) - base
+                                         : (a.cubic ? min(n, br[t].idx + 3) - base : 2);
                     for (int u = 0; u < cnt; ++u) {
                         const size_t off = (size_t)i * n + base + u;
                         if (a.sig) {
@@ -302,7 +342,8 @@ __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
                             tmp[u] = a.sig_iq[off];
                         }
                     }
-                    out = SINC ? sinc_gather(tmp, base, n, br[t], tab) : lerp_gather<true>(tmp, base, br[t]);
+                    out = SINC ? sinc_gather(tmp, base, n, br[t], tab)
+                               : (a.cubic ? cubic_gather(tmp, base, n, br[t]) : lerp_gather<true>(tmp, base, br[t]));
                 }
             }
             tile[jj][slot] = out;
@@ -448,6 +489,7 @@ struct Pass2Args {
     uint32_t *y1;
     int32_t *e1, *ctrl;
     int m, n, mpad;
+    int cubic;                        // 4-tap Lagrange instead of the lerp (SINC off)
 };
 
 template <int L, int E, bool SINC>
@@ -499,7 +541,8 @@ __global__ void __launch_bounds__((1 << L) / E) k_fx_pass2_fft(Pass2Args a) {
             const int cnt = lower_bound_from(xa, m, q, g);
             b = bracket_from_count(xa, m, asc, q, cnt);
         }
-        const uint32_t v = SINC ? sinc_gather(row, 0, m, b, tab) : lerp_gather<false>(row, 0, b);
+        const uint32_t v = SINC ? sinc_gather(row, 0, m, b, tab)
+                                : (a.cubic ? cubic_gather(row, 0, m, b) : lerp_gather<false>(row, 0, b));
         // window_fixed: cw = (int16)((hr * hc) >> 15); out = (int16)((x * cw) >> 15)
         const int cw = wrap16((hr * a.hamc[k]) >> 15);
         const int wr = wrap16((lo16(v) * cw) >> 15);
@@ -573,7 +616,8 @@ __global__ void __launch_bounds__((1 << L) / E) k_fx_fft2(Fft2Args a) {
 // ------------------------------------------------------------------------------------------ K4
 // img[j][k] = floor(sqrt(re^2 + im^2)) of sat16(y2[k][j] >> (emax2 - e2[k])); 64x64 tiles.
 __global__ void __launch_bounds__(256) k_fx_detect(const uint32_t *__restrict__ y2, const int32_t *__restrict__ e2,
-                                                   const int32_t *__restrict__ ctrl, uint16_t *__restrict__ img, int G) {
+                                                   const int32_t *__restrict__ ctrl, uint16_t *__restrict__ img, int G,
+                                                   int fused) {
     __shared__ uint16_t t[64][65];
     const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
     const int emax2 = ctrl[2];
@@ -590,11 +634,15 @@ __global__ void __launch_bounds__(256) k_fx_detect(const uint32_t *__restrict__ 
 #pragma unroll
     for (int u = 0; u < 16; ++u) {
         const int sh = min(emax2 - s[u], 31);
-        const int r = lo16(v[u]) >> sh, i = hi16(v[u]) >> sh;     // an arithmetic shift keeps int16 range
+        // emulator order: renormalise the pair, then |z|; fused (silicon) order: |z| of the row at its
+        // own exponent, then the magnitude shifted (model_detect_fusion.order_B_fused)
+        const int ps = fused ? 0 : sh;
+        const int r = lo16(v[u]) >> ps, i = hi16(v[u]) >> ps;     // an arithmetic shift keeps int16 range
         const unsigned p = (unsigned)(r * r) + (unsigned)(i * i);
         unsigned q = (unsigned)sqrtf((float)p);
         while (q * q > p) --q;
         while ((q + 1) * (q + 1) <= p) ++q;
+        if (fused) q >>= sh;
         t[tx][ty + 4 * u] = (uint16_t)min(q, 65535u);
     }
     __syncthreads();
@@ -633,7 +681,7 @@ struct FixedLaunch {
         if ((e = pf.mark(st, "q0max")) != cudaSuccess) return e;
         // K1: pass 1
         Pass1Args p1{reinterpret_cast<const float2 *>(sig), sig_iq, d.f0, d.df, d.fac, d.krp, d.order, d.sinc,
-                     d.ctrl, d.p1, d.m, d.n, d.mpad};
+                     d.ctrl, d.p1, d.m, d.n, d.mpad, d.range_cubic};
         dim3 g1((d.m + P1_SLOTS - 1) / P1_SLOTS, (d.n + P1_BINS - 1) / P1_BINS);
         if (d.range_sinc) {
             e = cudaFuncSetAttribute(k_fx_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p1_smem(true));
@@ -646,7 +694,8 @@ struct FixedLaunch {
         }
         if ((e = pf.mark(st, "pass1")) != cudaSuccess) return e;
         // K2: pass 2 + window + FFT-1
-        Pass2Args p2{d.p1, d.tan_s, d.krp, d.kcp, d.hamr, d.hamc, d.tw, d.sinc, d.y1, d.e1, d.ctrl, d.m, d.n, d.mpad};
+        Pass2Args p2{d.p1, d.tan_s, d.krp, d.kcp, d.hamr, d.hamc, d.tw, d.sinc, d.y1, d.e1, d.ctrl, d.m, d.n, d.mpad,
+                     d.az_cubic};
         const size_t s2 = pass2_smem(d.m, d.az_sinc != 0);
         if (d.az_sinc) {
             e = cudaFuncSetAttribute(k_fx_pass2_fft<L, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);
@@ -667,7 +716,7 @@ struct FixedLaunch {
         if ((e = pf.mark(st, "fft2")) != cudaSuccess) return e;
         // K4: renorm + detect + transpose
         dim3 g4(N / 64, N / 64);
-        k_fx_detect<<<g4, 256, 0, st>>>(d.y2, d.e2, d.ctrl, img, N);
+        k_fx_detect<<<g4, 256, 0, st>>>(d.y2, d.e2, d.ctrl, img, N, d.fused_detect);
         if ((e = pf.mark(st, "renorm_detect")) != cudaSuccess) return e;
         return cudaGetLastError();
     }

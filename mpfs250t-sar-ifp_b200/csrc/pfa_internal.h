@@ -15,6 +15,8 @@ namespace pfa {
 struct FixedDev {
     int m = 0, n = 0, G = 0, L = 0, mpad = 0;
     int range_sinc = 0, az_sinc = 0;
+    int range_cubic = 0, az_cubic = 0;      // 4-tap Lagrange variant (sinc flags off)
+    int fused_detect = 0;                   // silicon detect order
     // job vectors (device)
     float *f0 = nullptr, *df = nullptr, *fac = nullptr, *tan_s = nullptr;
     float *krp = nullptr, *kcp = nullptr;

@@ -93,8 +93,9 @@ extern "C" pfa_status pfa_form_fixed_noalloc(const pfa_config *cfg, const pfa_fi
     if (!cfg || !job || !sig_dev || !img_dev) return PFA_ERR_BAD_ARG;
     const pfa_config c = *cfg;
     if (c.mode != PFA_MODE_FIXED) return PFA_ERR_BAD_CONFIG;
-    if ((c.range_interp != PFA_INTERP_LERP && c.range_interp != PFA_INTERP_SINC) ||
-        (c.az_interp != PFA_INTERP_LERP && c.az_interp != PFA_INTERP_SINC))
+    if ((c.range_interp != PFA_INTERP_LERP && c.range_interp != PFA_INTERP_SINC && c.range_interp != PFA_INTERP_CUBIC) ||
+        (c.az_interp != PFA_INTERP_LERP && c.az_interp != PFA_INTERP_SINC && c.az_interp != PFA_INTERP_CUBIC) ||
+        (c.detect_order != PFA_DETECT_ORDER_EMULATOR && c.detect_order != PFA_DETECT_ORDER_FUSED))
         return PFA_ERR_BAD_CONFIG;
     if (c.m < 2 || c.n < 2 || c.grid < c.m || c.grid < c.n) return PFA_ERR_BAD_DIMS;
     if (c.grid > kMaxGrid) {
@@ -138,6 +139,9 @@ extern "C" pfa_status pfa_form_fixed_noalloc(const pfa_config *cfg, const pfa_fi
     d.m = m; d.n = n; d.G = G; d.L = L; d.mpad = (m + 31) / 32 * 32;
     d.range_sinc = c.range_interp == PFA_INTERP_SINC;
     d.az_sinc = c.az_interp == PFA_INTERP_SINC;
+    d.range_cubic = c.range_interp == PFA_INTERP_CUBIC;
+    d.az_cubic = c.az_interp == PFA_INTERP_CUBIC;
+    d.fused_detect = c.detect_order == PFA_DETECT_ORDER_FUSED;
     d.f0 = reinterpret_cast<float *>(base + Lt::f0);
     d.df = reinterpret_cast<float *>(base + Lt::df);
     d.fac = reinterpret_cast<float *>(base + Lt::fac);

@@ -13,7 +13,8 @@ LIB_PATH = Path(os.environ.get("PFA_B200_LIB", Path(__file__).resolve().parent /
 
 OK, BAD_CONFIG, BAD_DIMS, BAD_ARG, NOT_READY, CUDA, ALLOC, TIMEOUT, NO_DEVICE, TOO_LARGE = range(10)
 MODE_FIXED, MODE_FLOAT32, MODE_MIXED = 0, 1, 2
-LERP, SINC = 0, 1
+LERP, SINC, CUBIC = 0, 1, 2
+DETECT_ORDER_EMULATOR, DETECT_ORDER_FUSED = 0, 1
 LAYOUT_CENTRED, LAYOUT_NATURAL = 0, 1
 DETECT_MAG, DETECT_POWER, DETECT_COMPLEX = 0, 1, 2
 
@@ -31,7 +32,8 @@ class PfaError(RuntimeError):
 class Config(C.Structure):
     _fields_ = [("mode", C.c_int32), ("m", C.c_int32), ("n", C.c_int32), ("grid", C.c_int32),
                 ("range_interp", C.c_int32), ("az_interp", C.c_int32), ("device", C.c_int32),
-                ("fft_ept_cross", C.c_int32), ("fft_ept_range", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("fft_ept_cross", C.c_int32), ("fft_ept_range", C.c_int32), ("detect_order", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 class FixedJob(C.Structure):

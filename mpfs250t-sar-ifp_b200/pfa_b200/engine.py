@@ -97,10 +97,18 @@ class _Plan:
 class FixedPlan(_Plan):
     """Bit-exact fixed-point frame former for an (m, n) scene on a (grid, grid) raster."""
 
-    def __init__(self, m: int, n: int, grid: int, range_sinc: bool = False, az_sinc: bool = False, device: int = 0):
-        cfg = _lib.Config(mode=_lib.MODE_FIXED, m=m, n=n, grid=grid,
-                          range_interp=_lib.SINC if range_sinc else _lib.LERP,
-                          az_interp=_lib.SINC if az_sinc else _lib.LERP, device=device)
+    INTERP = {"lerp": _lib.LERP, "sinc": _lib.SINC, "cubic": _lib.CUBIC}
+    DETECT_ORDER = {"emulator": _lib.DETECT_ORDER_EMULATOR, "fused": _lib.DETECT_ORDER_FUSED}
+
+    def __init__(self, m: int, n: int, grid: int, range_sinc: bool = False, az_sinc: bool = False, device: int = 0,
+                 range_interp: str | None = None, az_interp: str | None = None, detect_order: str = "emulator"):
+        """``range_interp`` / ``az_interp`` ("lerp", "sinc", "cubic") override the two flags; "cubic" and
+        ``detect_order="fused"`` are the silicon A/B variants (gen_resample_vectors.gather_cubic,
+        model_detect_fusion.order_B_fused)."""
+        ri = self.INTERP[range_interp or ("sinc" if range_sinc else "lerp")]
+        ai = self.INTERP[az_interp or ("sinc" if az_sinc else "lerp")]
+        cfg = _lib.Config(mode=_lib.MODE_FIXED, m=m, n=n, grid=grid, range_interp=ri, az_interp=ai, device=device,
+                          detect_order=self.DETECT_ORDER[detect_order])
         super().__init__(cfg)
         self.m, self.n, self.grid, self.device = m, n, grid, device
 

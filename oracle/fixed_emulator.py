@@ -185,6 +185,45 @@ def gather_sinc(src_re, src_im, idx, wq, sn):
     return np.where(interior, sr, lr), np.where(interior, si, li)
 
 
+def lagrange_taps_q15(w):
+    """4-point cubic Lagrange taps at mu = w / 2^15 in Q15 (gen_resample_vectors.lagrange_taps_q15,
+    mpfs/fpga/tb/gen_resample_vectors.py:177-195): exact rationals, one round-half-up per tap.
+    Vectorised over integer w; each tap is floor((2 N + D) / (2 D)) with N/D the exact value x 2^15."""
+    w = np.asarray(w, np.int64)
+    a, b = w + 32768, w - 32768
+    c = w - 65536
+    nums = (-(w * b * c), a * b * c, -(a * w * c), a * w * b)
+    dens = (6 << 30, 1 << 31, 1 << 31, 6 << 30)
+    return np.stack([(2 * nn + d) // (2 * d) for nn, d in zip(nums, dens)], -1)
+
+
+def gather_cubic(src_re, src_im, idx, wq, sn):
+    """4-tap cubic Lagrange gather (gen_resample_vectors.gather_cubic, :298-325): taps at idx-1..idx+2
+    where 1 <= idx <= sn-3, sum >> 15 (floor), sat16; other live brackets use the integer 2-tap lerp
+    (no saturation needed: it stays between its two samples); idx < 0 gives 0."""
+    lr, li = gather_lerp(src_re, src_im, idx, wq)
+    interior = (idx >= 1) & (idx <= sn - 3)
+    if not interior.any():
+        return lr, li
+    base = np.where(interior, idx - 1, 0)
+    coef = lagrange_taps_q15(np.where(interior, wq, 0))
+    acc_r = np.zeros(idx.shape, np.int64)
+    acc_i = np.zeros(idx.shape, np.int64)
+    for t in range(4):
+        pos = base + t
+        acc_r += coef[..., t] * np.take_along_axis(src_re, pos, -1)
+        acc_i += coef[..., t] * np.take_along_axis(src_im, pos, -1)
+    return np.where(interior, sat16(acc_r >> 15), lr), np.where(interior, sat16(acc_i >> 15), li)
+
+
+def _gather(mode, src_re, src_im, idx, wq, sn, f32_product):
+    if mode == "sinc":
+        return gather_sinc(src_re, src_im, idx, wq, sn)
+    if mode == "cubic":
+        return gather_cubic(src_re, src_im, idx, wq, sn)
+    return gather_lerp(src_re, src_im, idx, wq, f32_product=f32_product)
+
+
 # ----------------------------------------------------------------------------- geometry
 def fixed_geometry(tables: dict, grid: int) -> dict:
     """Per-pulse fixed-point geometry (silicon_emulator.py:131-141), NumPy-2 dtype rules included."""
@@ -221,12 +260,16 @@ def pass1_coords(geo: dict, i: int) -> np.ndarray:
 
 
 # ----------------------------------------------------------------------------- resample
-def resample_two_pass(sig_re, sig_im, geo, range_sinc=False, az_sinc=False):
+def resample_two_pass(sig_re, sig_im, geo, range_sinc=False, az_sinc=False, range_mode=None, az_mode=None):
     """resample_fixed (silicon_emulator.py:125-156).
 
     Returns g2 planes of shape (grid, grid): rows = range bins, cols = cross bins; and the
     pass-1 scratch planes (grid, grid) rows = tan(phi)-sorted pulse slots, cols = range bins.
+    ``range_mode`` / ``az_mode`` ("lerp", "sinc", "cubic") override the two booleans; the cubic
+    variant is gen_resample_vectors.gather_cubic in both passes (integer edge lerp in pass 1 too).
     """
+    rmode = range_mode or ("sinc" if range_sinc else "lerp")
+    amode = az_mode or ("sinc" if az_sinc else "lerp")
     m, n, G = geo["m"], geo["n"], geo["grid"]
     if G < m or G < n:
         raise ValueError(f"grid {G} smaller than scene {m}x{n}")
@@ -234,10 +277,7 @@ def resample_two_pass(sig_re, sig_im, geo, range_sinc=False, az_sinc=False):
     s1i = np.zeros((G, G), np.int64)
     for i in range(m):
         idx, wq = bracket_q15(geo["KRp"], pass1_coords(geo, i))
-        if range_sinc:
-            r, im = gather_sinc(sig_re[i], sig_im[i], idx, wq, n)
-        else:
-            r, im = gather_lerp(sig_re[i], sig_im[i], idx, wq, f32_product=True)
+        r, im = _gather(rmode, sig_re[i], sig_im[i], idx, wq, n, True)
         s1r[geo["inv_order"][i]] = r
         s1i[geo["inv_order"][i]] = im
     tr = s1r.T
@@ -249,10 +289,7 @@ def resample_two_pass(sig_re, sig_im, geo, range_sinc=False, az_sinc=False):
         idx, wq = bracket_q15(geo["KCp"], src)
         row_r = np.ascontiguousarray(tr[j, :m])
         row_i = np.ascontiguousarray(ti[j, :m])
-        if az_sinc:
-            r, im = gather_sinc(row_r, row_i, idx, wq, m)
-        else:
-            r, im = gather_lerp(row_r, row_i, idx, wq)
+        r, im = _gather(amode, row_r, row_i, idx, wq, m, False)
         g2r[j] = r
         g2i[j] = im
     return g2r, g2i, s1r, s1i
@@ -341,8 +378,8 @@ def fft_bfp_rows(xr, xi, tw=None):
     return xr, xi, e
 
 
-def fft_pass(xr, xi, tw=None, chunk=1024):
-    """fft_pass_bfp (silicon_emulator.py:198-205): per-row BFP FFT, then >> (emax - e_row), sat16."""
+def fft_pass_raw(xr, xi, tw=None, chunk=1024):
+    """The per-row BFP FFTs of fft_pass_bfp before the global renormalisation: (y_re, y_im, e_row)."""
     R, n = xr.shape
     yr = np.empty_like(xr)
     yi = np.empty_like(xi)
@@ -350,6 +387,12 @@ def fft_pass(xr, xi, tw=None, chunk=1024):
     for r0 in range(0, R, chunk):
         r1 = min(R, r0 + chunk)
         yr[r0:r1], yi[r0:r1], e[r0:r1] = fft_bfp_rows(xr[r0:r1], xi[r0:r1], tw)
+    return yr, yi, e
+
+
+def fft_pass(xr, xi, tw=None, chunk=1024):
+    """fft_pass_bfp (silicon_emulator.py:198-205): per-row BFP FFT, then >> (emax - e_row), sat16."""
+    yr, yi, e = fft_pass_raw(xr, xi, tw, chunk)
     emax = int(e.max())
     sh = (emax - e)[:, None]
     return sat16(yr >> sh), sat16(yi >> sh), e
@@ -364,21 +407,39 @@ def detect_q(re, im):
     return np.clip(mag, 0, 0xFFFF).astype(np.uint16)
 
 
+def detect_fused(yr, yi, e):
+    """Silicon-order detect (model_detect_fusion.order_B_fused, mpfs/host/model_detect_fusion.py:56-71):
+    the magnitude at each row's native exponent, then the (emax - e_row) shift of the magnitude:
+    floor(sqrt(re^2 + im^2) / 2^s), clipped to uint16.  For these integer inputs this is
+    isqrt(re^2 + im^2) >> s (the float64 sqrt of an integer < 2^53 never rounds across an integer)."""
+    emax = int(e.max())
+    sh = (emax - e)[:, None]
+    mag = np.floor(np.sqrt((yr * yr + yi * yi).astype(np.float64))).astype(np.int64)
+    return np.clip(mag >> sh, 0, 0xFFFF).astype(np.uint16)
+
+
 # ----------------------------------------------------------------------------- whole frame
-def form_image(signal, tables, grid, range_sinc=False, az_sinc=False, keep=False):
+def form_image(signal, tables, grid, range_sinc=False, az_sinc=False, keep=False, range_mode=None, az_mode=None,
+               detect_order="emulator"):
     """The datapath of silicon_emulator.form_image after the CPHD read (:226-249).
 
-    Returns (img uint16 (grid, grid) [range bin][cross bin], diag dict).
+    Returns (img uint16 (grid, grid) [range bin][cross bin], diag dict).  Variants for comparison with
+    board captures: ``range_mode``/``az_mode`` "cubic" (gen_resample_vectors.gather_cubic) and
+    ``detect_order`` "fused" (detect at the native row exponent, model_detect_fusion.order_B_fused).
     """
     sr, si, q0e = quantize_q0(np.asarray(signal, np.complex64))
     geo = fixed_geometry(tables, grid)
     m, n = geo["m"], geo["n"]
-    g2r, g2i, s1r, s1i = resample_two_pass(sr, si, geo, range_sinc, az_sinc)
+    g2r, g2i, s1r, s1i = resample_two_pass(sr, si, geo, range_sinc, az_sinc, range_mode, az_mode)
     wr, wi = window_q15(g2r, g2i, m, n)
     tw = twiddles_q15(grid)
     y1r, y1i, e1 = fft_pass(wr, wi, tw)
-    y2r, y2i, e2 = fft_pass(np.ascontiguousarray(y1r.T), np.ascontiguousarray(y1i.T), tw)
-    img = detect_q(y2r.T, y2i.T)
+    if detect_order == "fused":
+        y2r, y2i, e2 = fft_pass_raw(np.ascontiguousarray(y1r.T), np.ascontiguousarray(y1i.T), tw)
+        img = np.ascontiguousarray(detect_fused(y2r, y2i, e2).T)
+    else:
+        y2r, y2i, e2 = fft_pass(np.ascontiguousarray(y1r.T), np.ascontiguousarray(y1i.T), tw)
+        img = detect_q(y2r.T, y2i.T)
     diag = dict(q0_exp=q0e, e_range=e1, e_az=e2, geo=geo)
     if keep:
         diag.update(q_re=sr, q_im=si, s1=(s1r, s1i), g2=(g2r, g2i), win=(wr, wi), y1=(y1r, y1i),

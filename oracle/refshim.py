@@ -57,7 +57,8 @@ _MODS = None
 
 def modules():
     """Return a namespace with the reference modules: ref (form_image_pfa), emu (silicon_emulator),
-    fx (fixedpoint), pipe (sar_pipeline), ser (serialize_inputs), grv (gen_resample_vectors), accel."""
+    fx (fixedpoint), pipe (sar_pipeline), ser (serialize_inputs), grv (gen_resample_vectors), accel,
+    mdf (model_detect_fusion)."""
     global _MODS
     if _MODS is not None:
         return _MODS
@@ -76,7 +77,8 @@ def modules():
         import silicon_emulator as emu        # noqa: E402
         import gen_resample_vectors as grv    # noqa: E402
         import accel                          # noqa: E402
-    _MODS = types.SimpleNamespace(ref=ref, fx=fx, pipe=pipe, ser=ser, emu=emu, grv=grv, accel=accel)
+        import model_detect_fusion as mdf     # noqa: E402
+    _MODS = types.SimpleNamespace(ref=ref, fx=fx, pipe=pipe, ser=ser, emu=emu, grv=grv, accel=accel, mdf=mdf)
     return _MODS
 
 

@@ -15,6 +15,10 @@ Outputs (JSON, a few KB):
   fft_kat.json       CRC-32 of the reference's CoreFFT BFP golden vectors (mpfs/host/corefft_vectors,
                      model ``fixedpoint.fft1d_bfp``, 16-bit data, 18-bit twiddles) per stimulus, plus
                      the manifest's exponents; the oracle's restated BFP FFT is pinned against them.
+  variants.json      CRC-32 of gen_resample_vectors.lagrange_taps_q15 over every Q15 weight, of
+                     gen_resample_vectors.gather_cubic and of model_detect_fusion.order_B_fused on
+                     seeded operands (``variant_inputs``): the cubic interpolator and the
+                     silicon-order detect the engine offers as variants.
   big_frames.json    (--big) the Centerfield-shaped full frame.
 """
 from __future__ import annotations
@@ -109,6 +113,36 @@ def fft_kat():
     return out
 
 
+def variant_inputs():
+    """Seeded operands of the variant pins (regenerated identically by the tests)."""
+    rng = np.random.default_rng(20261203)
+    sn = 300
+    src_re = rng.integers(-32768, 32768, sn)
+    src_im = rng.integers(-32768, 32768, sn)
+    idx = rng.integers(-3, sn - 1, 4000)
+    idx = np.where(idx < 0, -1, np.minimum(idx, sn - 2))
+    wq = rng.integers(0, 32768, 4000)
+    y_re = rng.integers(-32768, 32768, (32, 128))
+    y_im = rng.integers(-32768, 32768, (32, 128))
+    e = rng.integers(0, 12, 32)
+    return dict(sn=sn, src_re=src_re, src_im=src_im, idx=idx, wq=wq, y_re=y_re, y_im=y_im, e=e)
+
+
+def variants():
+    """The silicon A/B variants the engine also implements: gen_resample_vectors.lagrange_taps_q15 for
+    every Q15 weight, gen_resample_vectors.gather_cubic and model_detect_fusion.order_B_fused."""
+    m = refshim.modules()
+    taps = np.asarray([m.grv.lagrange_taps_q15(w) for w in range(32768)], np.int64)
+    v = variant_inputs()
+    src = [((int(i) & 0xFFFF) << 16) | (int(r) & 0xFFFF) for r, i in zip(v["src_re"], v["src_im"])]
+    words = m.grv.gather_cubic(src, [int(x) for x in v["idx"]], [int(x) for x in v["wq"]], v["sn"])
+    fused = m.mdf.order_B_fused(v["y_re"] + 1j * v["y_im"], v["e"])
+    return dict(lagrange_taps_crc=crc(taps.astype("<i4")),
+                lagrange_taps_w16384=[int(t) for t in taps[16384]],
+                gather_cubic_crc=crc(np.asarray(words, "<u4")),
+                detect_fused_crc=crc(np.asarray(fused, "<u2")))
+
+
 def big_cases():
     out = {}
     for name, wl, grid, rs, az in BIG_CASES:
@@ -132,6 +166,7 @@ def main():
         (HERE / "fixed_frames.json").write_text(json.dumps(dict(env=env, cases=fixed_cases()), indent=1))
         (HERE / "float_frames.json").write_text(json.dumps(dict(env=env, cases=float_cases()), indent=1))
         (HERE / "fft_kat.json").write_text(json.dumps(fft_kat(), indent=1))
+        (HERE / "variants.json").write_text(json.dumps(variants(), indent=1))
     if a.big or a.only_big:
         (HERE / "big_frames.json").write_text(json.dumps(dict(env=env, cases=big_cases()), indent=1))
 

@@ -50,6 +50,18 @@ def test_plan_create_rejects_bad_args_without_gpu():
     assert lib.pfa_form_fixed(None, None, None, None) == _lib.BAD_ARG
 
 
+def test_variant_configs_validated_without_gpu():
+    """The cubic resampler and the fused detect order are fixed-mode variants: float plans asking for
+    them, and unknown values, are refused before any device is touched."""
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    for kw in (dict(mode=_lib.MODE_FLOAT32, range_interp=_lib.CUBIC), dict(mode=_lib.MODE_MIXED, az_interp=_lib.CUBIC),
+               dict(mode=_lib.MODE_FLOAT32, detect_order=_lib.DETECT_ORDER_FUSED),
+               dict(mode=_lib.MODE_FIXED, grid=256, range_interp=3), dict(mode=_lib.MODE_FIXED, grid=256, detect_order=2)):
+        cfg = _lib.Config(m=200, n=200, **kw)
+        assert lib.pfa_plan_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.BAD_CONFIG, kw
+
+
 def test_product_sinc_table_equals_oracle():
     assert np.array_equal(tables.sinc_table_q15().astype(np.int64), fe.sinc_table_q15())
 

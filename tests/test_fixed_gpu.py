@@ -185,3 +185,18 @@ def test_caller_sinc_table(torch_cuda):
         with pytest.raises(_lib.PfaError) as ei:
             plan.set_job(job)
         assert ei.value.status == _lib.BAD_ARG
+
+
+@pytest.mark.parametrize("rmode,amode,order", [("cubic", "cubic", "emulator"), ("cubic", "sinc", "fused"),
+                                               ("lerp", "cubic", "fused"), ("sinc", "sinc", "fused")])
+def test_silicon_variants_bit_exact(torch_cuda, rmode, amode, order):
+    """The A/B variants (cubic Lagrange resampler, silicon detect order) against the oracle restating
+    gen_resample_vectors.gather_cubic and model_detect_fusion.order_B_fused, bit for bit."""
+    sc = synth.make_scene(230, 210, n_targets=8, snr_db=20.0, seed=41, jitter=0.3)
+    tb = geometry.prepare_tables_from_scene(sc)
+    ref, _ = fe.form_image(sc.signal, tb, 256, range_mode=rmode, az_mode=amode, detect_order=order)
+    with engine.FixedPlan(230, 210, 256, range_interp=rmode, az_interp=amode, detect_order=order) as plan:
+        plan.set_tables(tb)
+        img = plan.form(sc.signal)
+    assert np.array_equal(img, ref), f"{(img != ref).sum()} pixels differ"
+

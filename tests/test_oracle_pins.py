@@ -116,3 +116,44 @@ def test_prepare_tables_matches_reference(ref_modules):
     for k in ("ax", "ay", "freq", "KR", "KC", "tan_phi", "window"):
         assert np.array_equal(np.asarray(t0[k]), np.asarray(t1[k])), k
     assert t0["sgn"] == t1["sgn"] and tuple(t0["dims"]) == tuple(t1["dims"])
+
+
+# ----------------------------------------------------------------------------- silicon A/B variants
+def _variant_inputs():
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).parent / "golden"))
+    import make_golden
+    return make_golden.variant_inputs()
+
+
+def test_cubic_taps_and_gather_match_reference_vectors(golden_dir):
+    g = json.loads((golden_dir / "variants.json").read_text())
+    taps = fe.lagrange_taps_q15(np.arange(32768))
+    assert _crc(taps.astype("<i4")) == g["lagrange_taps_crc"]
+    assert list(taps[16384]) == g["lagrange_taps_w16384"]
+    v = _variant_inputs()
+    rr, ri = fe.gather_cubic(v["src_re"], v["src_im"], v["idx"], v["wq"], v["sn"])
+    words = ((ri.astype(np.int64) & 0xFFFF) << 16) | (rr.astype(np.int64) & 0xFFFF)
+    assert _crc(words.astype("<u4")) == g["gather_cubic_crc"]
+
+
+def test_fused_detect_matches_reference_vectors(golden_dir):
+    g = json.loads((golden_dir / "variants.json").read_text())
+    v = _variant_inputs()
+    img = fe.detect_fused(v["y_re"], v["y_im"], v["e"])
+    assert _crc(img.astype("<u2")) == g["detect_fused_crc"]
+
+
+def test_variant_frames_are_consistent():
+    """Frame level: the cubic variant differs from lerp only inside the cubic's interior, and the fused
+    detect stays within a few counts of the emulator order."""
+    sc = synth.make_scene(96, 80, n_targets=6, snr_db=20.0, seed=31)
+    tb = geometry.prepare_tables_from_scene(sc)
+    lerp, _ = fe.form_image(sc.signal, tb, 128, range_mode="lerp", az_mode="lerp")
+    cub, _ = fe.form_image(sc.signal, tb, 128, range_mode="cubic", az_mode="cubic")
+    assert (lerp > 0).sum() > 0 and not np.array_equal(lerp, cub)
+    emu, _ = fe.form_image(sc.signal, tb, 128, True, True)
+    fused, _ = fe.form_image(sc.signal, tb, 128, True, True, detect_order="fused")
+    d = np.abs(emu.astype(np.int64) - fused.astype(np.int64))
+    assert d.max() <= 2 and (d > 0).any()
