@@ -564,7 +564,7 @@ cudaError_t launch_fft2(const FloatDev &d, void *out, int detect, float scale, c
 // lines of 256 points and more
 template <int L, bool SINC>
 cudaError_t pass2_tile(const FloatDev &d, cudaStream_t st) {
-    if constexpr (L >= 8) {
+    if constexpr (L >= 8 && L <= 13) {      // 2^L / 8 threads must stay within a CTA's 1024
         if (d.ept_cross == 8) return launch_pass2<L, 8, SINC>(d, st);
     }
     return launch_pass2<L, Cfg<L>::E, SINC>(d, st);
@@ -572,7 +572,7 @@ cudaError_t pass2_tile(const FloatDev &d, cudaStream_t st) {
 
 template <int L>
 cudaError_t fft2_tile(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st) {
-    if constexpr (L >= 8) {
+    if constexpr (L >= 8 && L <= 13) {
         if (d.ept_range == 8) return launch_fft2<L, 8>(d, out, detect, scale, st);
     }
     return launch_fft2<L, Cfg<L>::E>(d, out, detect, scale, st);
@@ -589,6 +589,7 @@ cudaError_t dispatch_pass2(const FloatDev &d, cudaStream_t st) {
         case 11: return pass2_tile<11, SINC>(d, st);
         case 12: return pass2_tile<12, SINC>(d, st);
         case 13: return pass2_tile<13, SINC>(d, st);
+        case 14: return pass2_tile<14, SINC>(d, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -603,6 +604,7 @@ cudaError_t dispatch_fft2(const FloatDev &d, void *out, int detect, float scale,
         case 11: return fft2_tile<11>(d, out, detect, scale, st);
         case 12: return fft2_tile<12>(d, out, detect, scale, st);
         case 13: return fft2_tile<13>(d, out, detect, scale, st);
+        case 14: return fft2_tile<14>(d, out, detect, scale, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -637,7 +639,7 @@ cudaError_t float_alloc(FloatDev &d, int m, int n) {
     d.m2 = 1 << d.Lm; d.n2 = 1 << d.Ln;
     d.mpad = (m + 31) / 32 * 32;
     d.npad = (n + kCT - 1) / kCT * kCT;
-    if (d.m2 < 64 || d.n2 < 64 || d.m2 > 8192 || d.n2 > 8192) return cudaErrorInvalidValue;
+    if (d.m2 < 64 || d.n2 < 64 || d.m2 > 16384 || d.n2 > 16384) return cudaErrorInvalidValue;
     cudaError_t e;
 #define TRY(x) do { e = (x); if (e != cudaSuccess) return e; } while (0)
     TRY(dal(&d.f0, m)); TRY(dal(&d.df, m)); TRY(dal(&d.flast, m)); TRY(dal(&d.pr, m)); TRY(dal(&d.tan_s, m)); TRY(dal(&d.order, m));
@@ -729,6 +731,7 @@ cudaError_t af_range(const FloatDev &d, cudaStream_t st) {
     switch (d.Ln) {
         case 6: return CALL(6); case 7: return CALL(7); case 8: return CALL(8); case 9: return CALL(9);
         case 10: return CALL(10); case 11: return CALL(11); case 12: return CALL(12); case 13: return CALL(13);
+        case 14: return CALL(14);
         default: return cudaErrorInvalidValue;
     }
 #undef CALL
@@ -739,6 +742,7 @@ cudaError_t af_cross(const FloatDev &d, cudaStream_t st) {
     switch (d.Lm) {
         case 6: return CALL(6); case 7: return CALL(7); case 8: return CALL(8); case 9: return CALL(9);
         case 10: return CALL(10); case 11: return CALL(11); case 12: return CALL(12); case 13: return CALL(13);
+        case 14: return CALL(14);
         default: return cudaErrorInvalidValue;
     }
 #undef CALL

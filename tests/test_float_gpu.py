@@ -142,3 +142,14 @@ def test_host_entry_point_and_errors(torch_cuda):
         assert np.array_equal(a, b)
         st = plan._lib.pfa_form_float(plan.handle, None, None, 0, None)
         assert st == _lib.BAD_ARG
+
+
+@pytest.mark.parametrize("m,n,rs", [(9000, 300, False), (300, 9000, True)])
+def test_16384_point_lines(torch_cuda, m, n, rs):
+    """Lines of 16384 points on either axis (the reference's NDSU scene, 8167 x 8999, pads its range
+    axis to 16384): FP32 against FP64."""
+    sc = synth.make_scene(m, n, n_targets=8, clutter_db=-10.0, snr_db=20.0, seed=m + n, jitter=0.2)
+    tb = geometry.prepare_tables_from_scene(sc)
+    cz = _run(sc.signal, tb, detect="complex", rs=rs, az=rs)
+    assert cz.shape == (geometry.pow2(m), geometry.pow2(n))
+    assert fp.rel_l2(cz, _f64_mixed(sc.signal, tb, rs, rs)) <= TOL
