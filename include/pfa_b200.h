@@ -139,7 +139,8 @@ pfa_status pfa_set_float_job(pfa_plan *plan, const pfa_float_job *job);
 
 /* Fixed-point frame from the complex64 phase history (m x n, interleaved re/im float32, device).
  * Replaces: silicon_emulator.form_image lines :226-249 (Q0 quantise .. detect_fixed).
- * img_dev: uint16 [G][G], rows = range bins, cols = cross bins (the emulator's natural order). */
+ * img_dev: uint16 [G][G], rows = range bins, cols = cross bins (the emulator's natural order).
+ * sig_dev must be 16-byte aligned, img_dev 4-byte aligned (PFA_ERR_BAD_ARG otherwise). */
 pfa_status pfa_form_fixed(pfa_plan *plan, const float *sig_dev, uint16_t *img_dev, void *stream);
 /* Same, from an already quantised int16 I/Q signal (m x n x 2, device): the board's sig.bin
  * (serialize_inputs.py:1-30, ddr_layout.quantize_iq16).  Replaces :233-249. */

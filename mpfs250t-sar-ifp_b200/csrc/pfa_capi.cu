@@ -289,6 +289,7 @@ static pfa_status fixed_common(pfa_plan *p, const float *sig, const int16_t *iq,
     if (!p->job_ready) return fail(p, PFA_ERR_NOT_READY, "pfa_set_fixed_job not called");
     if (sig && (reinterpret_cast<uintptr_t>(sig) & 15)) return fail(p, PFA_ERR_BAD_ARG, "signal must be 16-byte aligned");
     if (iq && (reinterpret_cast<uintptr_t>(iq) & 3)) return fail(p, PFA_ERR_BAD_ARG, "iq16 signal must be 4-byte aligned");
+    if (reinterpret_cast<uintptr_t>(img) & 3) return fail(p, PFA_ERR_BAD_ARG, "image must be 4-byte aligned");
     DeviceGuard dg(p->device);
     cudaError_t e = pfa::fixed_form(p->fx, sig, reinterpret_cast<const uint32_t *>(iq), img,
                                     reinterpret_cast<cudaStream_t>(stream), &p->prof);

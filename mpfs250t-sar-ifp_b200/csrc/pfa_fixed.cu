@@ -37,6 +37,13 @@ __device__ __forceinline__ int lo16(uint32_t p) { return (int)(int16_t)(p & 0xff
 __device__ __forceinline__ int hi16(uint32_t p) { return (int)(int16_t)(p >> 16); }
 __device__ __forceinline__ int wrap16(int v) { return (int)(int16_t)(v & 0xffff); }
 
+// Source samples are packed int16 I/Q words (pass-2 rows) or unpacked int32 pairs (pass-1 windows,
+// one 8-byte shared load per tap instead of a load and two sign extensions).
+__device__ __forceinline__ int re_of(uint32_t v) { return lo16(v); }
+__device__ __forceinline__ int im_of(uint32_t v) { return hi16(v); }
+__device__ __forceinline__ int re_of(int2 v) { return v.x; }
+__device__ __forceinline__ int im_of(int2 v) { return v.y; }
+
 // 16-byte global -> shared copies that complete asynchronously (both addresses 16-byte aligned)
 __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -116,44 +123,44 @@ __device__ __forceinline__ Bracket bracket_from_count(const F &xa, int n, bool a
 
 // 32-tap sinc / edge lerp / zero of apply_sinc (silicon_emulator.py:88-122) on a window of packed
 // int16x2 samples; `win` is indexed by (source index - base).
-__device__ __forceinline__ uint32_t sinc_gather(const uint32_t *win, int base, int sn, Bracket b,
-                                                const int16_t *tab) {
+template <class W>
+__device__ __forceinline__ uint32_t sinc_gather(const W *win, int base, int sn, Bracket b, const int16_t *tab) {
     if (b.idx < 0) return 0u;
     if (b.idx >= -kSincFirst && b.idx <= sn - (kSincTaps + kSincFirst)) {
         const int16_t *c = tab + (b.wq >> 7);           // table stored [tap][phase]: phases spread over banks
-        const uint32_t *x = win + (b.idx + kSincFirst - base);
+        const W *x = win + (b.idx + kSincFirst - base);
         // Two int32 half sums (taps 0-15, 16-31): the table is checked on upload to have
         // sum |tap| <= 65535 over each half of every phase, so |half sum| <= 32768 * 65535 < 2^31.
         int ar0 = 0, ai0 = 0, ar1 = 0, ai1 = 0;
 #pragma unroll
         for (int t = 0; t < kSincTaps / 2; ++t) {
             const int ct = c[t * 256];
-            const uint32_t v = x[t];
-            ar0 += ct * lo16(v);
-            ai0 += ct * hi16(v);
+            const W v = x[t];
+            ar0 += ct * re_of(v);
+            ai0 += ct * im_of(v);
         }
 #pragma unroll
         for (int t = kSincTaps / 2; t < kSincTaps; ++t) {
             const int ct = c[t * 256];
-            const uint32_t v = x[t];
-            ar1 += ct * lo16(v);
-            ai1 += ct * hi16(v);
+            const W v = x[t];
+            ar1 += ct * re_of(v);
+            ai1 += ct * im_of(v);
         }
         const long long ar = (long long)ar0 + ar1, ai = (long long)ai0 + ai1;
         return pack16((int)sat16ll((ar + (1 << 14)) >> 15), (int)sat16ll((ai + (1 << 14)) >> 15));
     }
-    const uint32_t va = win[b.idx - base], vb = win[b.idx + 1 - base];
-    const int ar = lo16(va), ai = hi16(va), br = lo16(vb), bi = hi16(vb);
+    const W va = win[b.idx - base], vb = win[b.idx + 1 - base];
+    const int ar = re_of(va), ai = im_of(va), br = re_of(vb), bi = im_of(vb);
     return pack16(sat16(ar + (((br - ar) * b.wq) >> 15)), sat16(ai + (((bi - ai) * b.wq) >> 15)));
 }
 
 // apply_fixed (silicon_emulator.py:60-71).  F32PROD: the product (b-a)*wq rounded to float32, as in
 // pass 1 where the emulator's quantised signal is complex64.
-template <bool F32PROD>
-__device__ __forceinline__ uint32_t lerp_gather(const uint32_t *win, int base, Bracket b) {
+template <bool F32PROD, class W>
+__device__ __forceinline__ uint32_t lerp_gather(const W *win, int base, Bracket b) {
     if (b.idx < 0) return 0u;
-    const uint32_t va = win[b.idx - base], vb = win[b.idx + 1 - base];
-    const int ar = lo16(va), ai = hi16(va), br = lo16(vb), bi = hi16(vb);
+    const W va = win[b.idx - base], vb = win[b.idx + 1 - base];
+    const int ar = re_of(va), ai = im_of(va), br = re_of(vb), bi = im_of(vb);
     int sr, si;
     if (F32PROD) {
         const float w = (float)b.wq;
@@ -186,17 +193,18 @@ __device__ __forceinline__ void lagrange_q15(int w, int (&c)[4]) {
 
 // gen_resample_vectors.gather_cubic (:298-325): taps at idx-1..idx+2 where 1 <= idx <= sn-3, sum >> 15
 // (floor), sat16; other live brackets take the integer 2-tap lerp; idx < 0 gives 0.
-__device__ __forceinline__ uint32_t cubic_gather(const uint32_t *win, int base, int sn, Bracket b) {
+template <class W>
+__device__ __forceinline__ uint32_t cubic_gather(const W *win, int base, int sn, Bracket b) {
     if (b.idx < 0) return 0u;
     if (b.idx >= 1 && b.idx <= sn - 3) {
         int c[4];
         lagrange_q15(b.wq, c);
-        const uint32_t *x = win + (b.idx - 1 - base);
+        const W *x = win + (b.idx - 1 - base);
         long long ar = 0, ai = 0;
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
-            ar += (long long)c[t] * lo16(x[t]);
-            ai += (long long)c[t] * hi16(x[t]);
+            ar += (long long)c[t] * re_of(x[t]);
+            ai += (long long)c[t] * im_of(x[t]);
         }
         return pack16((int)sat16ll(ar >> 15), (int)sat16ll(ai >> 15));
     }
@@ -223,7 +231,7 @@ __global__ void k_q0exp(int32_t *ctrl) { ctrl[3] = q0_exponent((uint32_t)ctrl[0]
 constexpr int P1_SLOTS = 32;          // sorted pulse slots per CTA
 constexpr int P1_BINS = 128;          // range bins per CTA
 constexpr int P1_WARPS = 8;
-constexpr int P1_WMAX = 384;          // per-warp source window (samples)
+constexpr int P1_WMAX = 256;          // per-warp source window (samples); wider windows gather from global
 
 struct Pass1Args {
     const float2 *sig;                // complex64 input (or nullptr)
@@ -238,14 +246,14 @@ struct Pass1Args {
 };
 
 constexpr size_t P1_SMEM_TILE = (size_t)P1_BINS * (P1_SLOTS + 1) * 4;
-constexpr size_t P1_SMEM_WIN = (size_t)P1_WARPS * P1_WMAX * 4;
+constexpr size_t P1_SMEM_WIN = (size_t)P1_WARPS * P1_WMAX * 8;   // int32 I/Q pairs
 constexpr size_t p1_smem(bool sinc) { return P1_SMEM_TILE + P1_SMEM_WIN + (sinc ? 2 * 256 * kSincTaps : 0); }
 
 template <bool SINC>
 __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t(*tile)[P1_SLOTS + 1] = reinterpret_cast<uint32_t(*)[P1_SLOTS + 1]>(smem);
-    uint32_t(*win)[P1_WMAX] = reinterpret_cast<uint32_t(*)[P1_WMAX]>(smem + P1_SMEM_TILE);
+    int2(*win)[P1_WMAX] = reinterpret_cast<int2(*)[P1_WMAX]>(smem + P1_SMEM_TILE);
     int16_t *tab = reinterpret_cast<int16_t *>(smem + P1_SMEM_TILE + P1_SMEM_WIN);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r0 = blockIdx.x * P1_SLOTS;
@@ -304,16 +312,17 @@ __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
             whi = min(n, hi_i + (SINC ? kSincTaps + kSincFirst : (a.cubic ? 3 : 2)));
         }
         const bool fits = (whi - wlo) <= P1_WMAX;
-        uint32_t *w = win[warp];
+        int2 *w = win[warp];
         if (fits) {
             for (int k = wlo + lane; k < whi; k += 32) {
                 const size_t off = (size_t)i * n + k;
-                uint32_t v;
+                int2 v;
                 if (a.sig) {
                     const float2 z = a.sig[off];
-                    v = pack16(q0_quantise(z.x, lsb), q0_quantise(z.y, lsb));
+                    v = make_int2(q0_quantise(z.x, lsb), q0_quantise(z.y, lsb));
                 } else {
-                    v = a.sig_iq[off];
+                    const uint32_t q = a.sig_iq[off];
+                    v = make_int2(lo16(q), hi16(q));
                 }
                 w[k - wlo] = v;
             }
@@ -614,39 +623,52 @@ __global__ void __launch_bounds__((1 << L) / E) k_fx_fft2(Fft2Args a) {
 }
 
 // ------------------------------------------------------------------------------------------ K4
-// img[j][k] = floor(sqrt(re^2 + im^2)) of sat16(y2[k][j] >> (emax2 - e2[k])); 64x64 tiles.
+// img[j][k] = floor(sqrt(re^2 + im^2)) of sat16(y2[k][j] >> (emax2 - e2[k])); 64 (k) x 128 (j) tiles,
+// two adjacent columns per thread (8-byte loads), two adjacent k per thread on the transposed store.
+__device__ __forceinline__ uint16_t detect_one(uint32_t v, int sh, int fused) {
+    // emulator order: renormalise the pair, then |z|; fused (silicon) order: |z| of the row at its own
+    // exponent, then the magnitude shifted (model_detect_fusion.order_B_fused)
+    const int ps = fused ? 0 : sh;
+    const int r = lo16(v) >> ps, i = hi16(v) >> ps;          // an arithmetic shift keeps int16 range
+    const unsigned p = (unsigned)(r * r) + (unsigned)(i * i);
+    unsigned q = (unsigned)sqrtf((float)p);
+    while (q * q > p) --q;
+    while ((q + 1) * (q + 1) <= p) ++q;
+    if (fused) q >>= sh;
+    return (uint16_t)min(q, 65535u);
+}
+
 __global__ void __launch_bounds__(256) k_fx_detect(const uint32_t *__restrict__ y2, const int32_t *__restrict__ e2,
                                                    const int32_t *__restrict__ ctrl, uint16_t *__restrict__ img, int G,
                                                    int fused) {
-    __shared__ uint16_t t[64][65];
-    const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+    __shared__ uint16_t t[128][65];
+    const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 128;
     const int emax2 = ctrl[2];
-    const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;   // 64 x 4
+    const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;   // 64 column pairs x 4 rows
     // all 16 loads of this thread in flight before any arithmetic
-    uint32_t v[16];
+    const bool live = j0 + 2 * tx < G;                        // G = 64: half a tile
+    uint2 v[16];
     int s[16];
 #pragma unroll
     for (int u = 0; u < 16; ++u) {
         const int k = k0 + ty + 4 * u;
-        v[u] = __ldcs(y2 + (size_t)k * G + j0 + tx);
+        v[u] = live ? __ldcs(reinterpret_cast<const uint2 *>(y2 + (size_t)k * G + j0) + tx) : make_uint2(0u, 0u);
         s[u] = __ldg(e2 + k);
     }
 #pragma unroll
     for (int u = 0; u < 16; ++u) {
         const int sh = min(emax2 - s[u], 31);
-        // emulator order: renormalise the pair, then |z|; fused (silicon) order: |z| of the row at its
-        // own exponent, then the magnitude shifted (model_detect_fusion.order_B_fused)
-        const int ps = fused ? 0 : sh;
-        const int r = lo16(v[u]) >> ps, i = hi16(v[u]) >> ps;     // an arithmetic shift keeps int16 range
-        const unsigned p = (unsigned)(r * r) + (unsigned)(i * i);
-        unsigned q = (unsigned)sqrtf((float)p);
-        while (q * q > p) --q;
-        while ((q + 1) * (q + 1) <= p) ++q;
-        if (fused) q >>= sh;
-        t[tx][ty + 4 * u] = (uint16_t)min(q, 65535u);
+        t[2 * tx][ty + 4 * u] = detect_one(v[u].x, sh, fused);
+        t[2 * tx + 1][ty + 4 * u] = detect_one(v[u].y, sh, fused);
     }
     __syncthreads();
-    for (int jj = ty; jj < 64; jj += 4) img[(size_t)(j0 + jj) * G + k0 + tx] = t[jj][tx];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll 4
+    for (int jj = w; jj < 128; jj += 8) {
+        if (j0 + jj >= G) break;
+        const uint32_t pair = (uint32_t)t[jj][2 * lane] | ((uint32_t)t[jj][2 * lane + 1] << 16);
+        reinterpret_cast<uint32_t *>(img + (size_t)(j0 + jj) * G + k0)[lane] = pair;
+    }
 }
 
 // ------------------------------------------------------------------------------------------ launch
@@ -715,7 +737,7 @@ struct FixedLaunch {
         k_fx_fft2<L, E><<<N, T, s3, st>>>(f2);
         if ((e = pf.mark(st, "fft2")) != cudaSuccess) return e;
         // K4: renorm + detect + transpose
-        dim3 g4(N / 64, N / 64);
+        dim3 g4((N + 127) / 128, N / 64);
         k_fx_detect<<<g4, 256, 0, st>>>(d.y2, d.e2, d.ctrl, img, N, d.fused_detect);
         if ((e = pf.mark(st, "renorm_detect")) != cudaSuccess) return e;
         return cudaGetLastError();

@@ -91,6 +91,7 @@ bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
 extern "C" pfa_status pfa_form_fixed_noalloc(const pfa_config *cfg, const pfa_fixed_job *job, const float *sig_dev,
                                              uint16_t *img_dev, void *stream) {
     if (!cfg || !job || !sig_dev || !img_dev) return PFA_ERR_BAD_ARG;
+    if ((reinterpret_cast<uintptr_t>(sig_dev) & 15) || (reinterpret_cast<uintptr_t>(img_dev) & 3)) return PFA_ERR_BAD_ARG;
     const pfa_config c = *cfg;
     if (c.mode != PFA_MODE_FIXED) return PFA_ERR_BAD_CONFIG;
     if ((c.range_interp != PFA_INTERP_LERP && c.range_interp != PFA_INTERP_SINC && c.range_interp != PFA_INTERP_CUBIC) ||
