@@ -126,21 +126,41 @@ __device__ __forceinline__ void mirror_frac(Frac &fr) {
     fr.rev = 1;
 }
 
-// lerp or float sinc of complex64 samples `src` (indexed from `base`) at bracket (j, frac)
+// Float sinc table: 256 phases x 32 taps / 32768, one phase per row of kTabStride floats.  A lane reads
+// its phase's taps four at a time (16-byte loads); the 36-float stride puts the rows of 8 consecutive
+// phases on distinct 4-bank groups, so a warp's 32 phases cost 4 wavefronts per load, the minimum.
+constexpr int kTabStride = 36;
+constexpr int kTabFloats = 256 * kTabStride;
+
+// lerp or float sinc of complex64 samples `src` (indexed from `base`) at bracket (j, frac); the sinc
+// sums the taps in natural order (t = 0..31) with fused multiply-adds
 template <bool SINC>
 __device__ __forceinline__ float2 gather_f32(const float2 *src, int base, int sn, int j, Frac fr,
                                              const float *tab) {
     if (j < 0) return make_float2(0.f, 0.f);
     const float frac = fr.f;
     if (SINC && j >= 15 && j <= sn - 17) {
-        const float *c = tab + fr.ph;                    // table stored [tap][phase]: phases spread over banks
+        const float4 *c4 = reinterpret_cast<const float4 *>(tab + fr.ph * kTabStride);
         const float2 *x = src + (j - 15 - base);
         float ar = 0.f, ai = 0.f;
+        if (!fr.rev) {
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
-            const float ct = fr.rev ? c[(31 - t) * 256] : c[t * 256];
-            ar = fmaf(ct, x[t].x, ar);
-            ai = fmaf(ct, x[t].y, ai);
+            for (int q = 0; q < 8; ++q) {
+                const float4 c = c4[q];
+                ar = fmaf(c.x, x[4 * q].x, ar);     ai = fmaf(c.x, x[4 * q].y, ai);
+                ar = fmaf(c.y, x[4 * q + 1].x, ar); ai = fmaf(c.y, x[4 * q + 1].y, ai);
+                ar = fmaf(c.z, x[4 * q + 2].x, ar); ai = fmaf(c.z, x[4 * q + 2].y, ai);
+                ar = fmaf(c.w, x[4 * q + 3].x, ar); ai = fmaf(c.w, x[4 * q + 3].y, ai);
+            }
+        } else {                                          // descending axis: tap 31 - t at sample t
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float4 c = c4[7 - q];
+                ar = fmaf(c.w, x[4 * q].x, ar);     ai = fmaf(c.w, x[4 * q].y, ai);
+                ar = fmaf(c.z, x[4 * q + 1].x, ar); ai = fmaf(c.z, x[4 * q + 1].y, ai);
+                ar = fmaf(c.y, x[4 * q + 2].x, ar); ai = fmaf(c.y, x[4 * q + 2].y, ai);
+                ar = fmaf(c.x, x[4 * q + 3].x, ar); ai = fmaf(c.x, x[4 * q + 3].y, ai);
+            }
         }
         return make_float2(ar, ai);
     }

@@ -35,7 +35,9 @@ template <int L, int E>
 using F32Fft = StockhamFft<L, E>;
 
 // ------------------------------------------------------------------------------------------ K1f
-constexpr int F1_SLOTS = 32, F1_BINS = 128, F1_WARPS = 8, F1_WMAX = 384;
+constexpr int F1_SLOTS = 32, F1_WARPS = 8, F1_WMAX = 256;
+// range bins per CTA: the sinc variant takes a narrower tile so three CTAs (with the 32 KB table) fit an SM
+constexpr int f1_bins(bool sinc) { return sinc ? 64 : 128; }
 
 struct FPass1Args {
     const float2 *sig;
@@ -48,20 +50,25 @@ struct FPass1Args {
 };
 
 constexpr size_t f1_smem(bool sinc) {
-    return (size_t)F1_BINS * (F1_SLOTS + 1) * 8 + (size_t)F1_WARPS * F1_WMAX * 8 + (sinc ? 256 * 32 * 4 : 0);
+    return (size_t)f1_bins(sinc) * (F1_SLOTS + 1) * 8 + (size_t)F1_WARPS * F1_WMAX * 8 + (sinc ? kTabFloats * 4 : 0);
 }
 
 template <bool SINC>
 __global__ void __launch_bounds__(256) k_fl_pass1(FPass1Args a) {
     extern __shared__ __align__(16) unsigned char smem[];
     float2(*tile)[F1_SLOTS + 1] = reinterpret_cast<float2(*)[F1_SLOTS + 1]>(smem);
+    constexpr int F1_BINS = f1_bins(SINC);
     float2(*win)[F1_WMAX] = reinterpret_cast<float2(*)[F1_WMAX]>(smem + (size_t)F1_BINS * (F1_SLOTS + 1) * 8);
     float *tab = reinterpret_cast<float *>(smem + (size_t)F1_BINS * (F1_SLOTS + 1) * 8 + (size_t)F1_WARPS * F1_WMAX * 8);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r0 = blockIdx.x * F1_SLOTS, j0 = blockIdx.y * F1_BINS;
     const int n = a.n;
-    if (SINC)
-        for (int i = tid; i < 256 * 32; i += blockDim.x) tab[i] = a.tabf[i];
+    if (SINC) {
+        const float4 *src = reinterpret_cast<const float4 *>(a.tabf);
+        float4 *dst = reinterpret_cast<float4 *>(tab);
+#pragma unroll
+        for (int i = 0; i < kTabFloats / 4 / 256; ++i) dst[tid + 256 * i] = __ldg(src + tid + 256 * i);
+    }
     __syncthreads();
     for (int s = 0; s < F1_SLOTS / F1_WARPS; ++s) {
         const int slot = warp + F1_WARPS * s;
@@ -190,7 +197,7 @@ k_fl_pass2_fft(FPass2Args a) {
         const int nchunk = (m + 1) >> 1;                      // 16-byte chunks (the pad covers odd m)
         for (int c = tid; c < nchunk; c += T) cp_async16(row + 2 * c, src + 2 * c);
         if (SINC)
-            for (int c = tid; c < 256 * 32 / 4; c += T) cp_async16(tab + 4 * c, a.tabf + 4 * c);
+            for (int c = tid; c < kTabFloats / 4; c += T) cp_async16(tab + 4 * c, a.tabf + 4 * c);
         cp_async_commit();
     }
     const double krj = a.kr_grid[j];
@@ -540,7 +547,7 @@ cudaError_t launch_pass2(const FloatDev &d, cudaStream_t st) {
     FPass2Args p{d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabf,
                  d.twm, d.y1, d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0};
     size_t regA = (std::max((size_t)8 * d.m, (size_t)8 * F::xbuf_elems()) + 15) & ~(size_t)15;
-    size_t sm = regA + (SINC ? 256 * 32 * 4 : 0);
+    size_t sm = regA + (SINC ? kTabFloats * 4 : 0);
     auto fn = k_fl_pass2_fft<L, E, SINC>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
@@ -645,7 +652,7 @@ cudaError_t float_alloc(FloatDev &d, int m, int n) {
     TRY(dal(&d.f0, m)); TRY(dal(&d.df, m)); TRY(dal(&d.flast, m)); TRY(dal(&d.pr, m)); TRY(dal(&d.tan_s, m)); TRY(dal(&d.order, m));
     TRY(dal(&d.kr, n)); TRY(dal(&d.kc, m)); TRY(dal(&d.ham_m64, m)); TRY(dal(&d.ham_n64, n));
     TRY(dal(&d.twm, d.m2)); TRY(dal(&d.twn, d.n2));
-    TRY(dal(&d.tabf, 256 * 32));
+    TRY(dal(&d.tabf, kTabFloats));
     TRY(dal(&d.p1, (size_t)n * d.mpad)); TRY(dal(&d.y1, (size_t)d.npad * d.m2));
 #undef TRY
     return cudaSuccess;
@@ -665,7 +672,7 @@ cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int dete
     cudaError_t e = pf.mark(st, "start");
     if (e != cudaSuccess) return e;
     FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabf, nullptr, d.p1, d.m, d.n, d.mpad};
-    dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + F1_BINS - 1) / F1_BINS);
+    dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + f1_bins(d.range_sinc) - 1) / f1_bins(d.range_sinc));
     if (d.range_sinc) {
         e = cudaFuncSetAttribute(k_fl_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1_smem(true));
         if (e != cudaSuccess) return e;
@@ -763,7 +770,7 @@ cudaError_t autofocus_grad(const FloatDev &d0, const float2 *sig, const float *t
     if ((e = cudaMemsetAsync(d.af_acc, 0, 2 * sizeof(double), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(d.af_dacc, 0, sizeof(float) * d.mpad, st)) != cudaSuccess) return e;
     FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabf, theta, d.p1, d.m, d.n, d.mpad};
-    dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + F1_BINS - 1) / F1_BINS);
+    dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + f1_bins(false) - 1) / f1_bins(false));
     e = cudaFuncSetAttribute(k_fl_pass1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1_smem(false));
     if (e != cudaSuccess) return e;
     k_fl_pass1<false><<<g1, 256, f1_smem(false), st>>>(p1);
@@ -823,9 +830,9 @@ pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *job) {
     std::vector<float2> twm, twn;
     pfa::full_twiddles(d.m2, twm);
     pfa::full_twiddles(d.n2, twn);
-    std::vector<float> tabf(256 * 32);
+    std::vector<float> tabf(pfa::kTabFloats, 0.0f);
     const int16_t *tq = pfa::builtin_sinc_table();
-    for (int i = 0; i < 256 * 32; ++i) tabf[(i & 31) * 256 + (i >> 5)] = (float)tq[i] / 32768.0f;   // [tap][phase]
+    for (int i = 0; i < 256 * 32; ++i) tabf[(i >> 5) * pfa::kTabStride + (i & 31)] = (float)tq[i] / 32768.0f;   // [phase][tap], padded rows
     cudaError_t e;
 #define CPY(dst, src, cnt) do { e = cudaMemcpy(dst, src, sizeof(*(dst)) * (cnt), cudaMemcpyHostToDevice); \
         if (e != cudaSuccess) return fcuda(p, e, "float job upload"); } while (0)
@@ -833,7 +840,7 @@ pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *job) {
     CPY(d.order, job->order, m); CPY(d.kr, job->kr_grid, n); CPY(d.kc, job->kc_grid, m);
     if (d.window) { CPY(d.ham_m64, job->ham_m, m); CPY(d.ham_n64, job->ham_n, n); }
     CPY(d.twm, twm.data(), d.m2); CPY(d.twn, twn.data(), d.n2);
-    CPY(d.tabf, tabf.data(), 256 * 32);
+    CPY(d.tabf, tabf.data(), pfa::kTabFloats);
 #undef CPY
     p->job_ready = true;
     return PFA_OK;

@@ -217,7 +217,7 @@ __global__ void __cluster_dims__(kMxCT, 1, 1) __launch_bounds__(Geo<L>::THREADS,
     unsigned char *b2 = smem + G::FN2_BYTES;                 // stage-2 operand, then the exchange line
     float2 *row = reinterpret_cast<float2 *>(b2 + G::B2_BYTES);
     float *tab = reinterpret_cast<float *>(b2 + G::B2_BYTES + row_bytes);
-    float *red = tab + (SINC ? 256 * 32 : 0);
+    float *red = tab + (SINC ? kTabFloats : 0);
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tbase;
     namespace cg = cooperative_groups;
@@ -232,7 +232,7 @@ __global__ void __cluster_dims__(kMxCT, 1, 1) __launch_bounds__(Geo<L>::THREADS,
     }
     F::load_fn2(a.fn2, fn2, tid);
     if (SINC)
-        for (int i = tid; i < 256 * 32; i += T) tab[i] = __ldg(a.tabf + i);
+        for (int i = tid; i < kTabFloats; i += T) tab[i] = __ldg(a.tabf + i);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -354,7 +354,7 @@ size_t fft2_smem() {
 template <int L, bool SINC>
 size_t pass2_smem(int m) {
     return std::max(kMxMinSmem, (size_t)Geo<L>::FN2_BYTES + Geo<L>::B2_BYTES + (((size_t)8 * m + 15) & ~(size_t)15) +
-                                    (SINC ? 256 * 32 * 4 : 0) + 64 * 4);
+                                    (SINC ? kTabFloats * 4 : 0) + 64 * 4);
 }
 
 template <int L>
