@@ -861,6 +861,8 @@ pfa_status pfa_form_float(pfa_plan *p, const float *sig_dev, void *out_dev, int3
     return PFA_OK;
 }
 
+static pfa_status mixed_timeout_check(pfa_plan *p);
+
 pfa_status pfa_form_float_host(pfa_plan *p, const float *sig_host, void *out_host, int32_t detect) {
     if (!p || !sig_host || !out_host) return PFA_ERR_BAD_ARG;
     if (p->cfg.mode != PFA_MODE_FLOAT32 && p->cfg.mode != PFA_MODE_MIXED) return ffail(p, PFA_ERR_BAD_CONFIG, "plan is not float mode");
@@ -889,7 +891,19 @@ pfa_status pfa_form_float_host(pfa_plan *p, const float *sig_host, void *out_hos
     if ((e = cudaMemcpyAsync(out_host, p->staging_out, out_b, cudaMemcpyDeviceToHost, p->host_stream)) != cudaSuccess)
         return fcuda(p, e, "d2h");
     if ((e = cudaStreamSynchronize(p->host_stream)) != cudaSuccess) return fcuda(p, e, "sync");
-    return PFA_OK;
+    return mixed_timeout_check(p);
+}
+
+// Mixed mode: a tensor-core completion wait that ran out sets a device flag; synchronous entry points read
+// (and clear) it after their frames and report PFA_ERR_TIMEOUT.
+static pfa_status mixed_timeout_check(pfa_plan *p) {
+    if (!p->fl.mixed || !p->fl.mx_err) return PFA_OK;
+    int flag = 0;
+    cudaError_t e = cudaMemcpy(&flag, p->fl.mx_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fcuda(p, e, "timeout flag");
+    if (!flag) return PFA_OK;
+    cudaMemset(p->fl.mx_err, 0, sizeof(int));
+    return ffail(p, PFA_ERR_TIMEOUT, "mixed mode: a tensor-core completion wait timed out (frame not valid)");
 }
 
 static pfa_status float_frame(pfa_plan *p, const void *in, void *out, cudaStream_t st, int32_t detect) {
@@ -904,8 +918,9 @@ pfa_status pfa_form_float_host_frames(pfa_plan *p, const float *const *sig_hosts
     DevGuard dg(p->device);
     const size_t in_b = sizeof(float) * 2 * (size_t)p->fl.m * p->fl.n;
     const size_t out_b = (detect == PFA_DETECT_COMPLEX ? 8 : 4) * (size_t)p->fl.m2 * p->fl.n2;
-    return pfa::run_host_frames(p, reinterpret_cast<const void *const *>(sig_hosts), out_hosts, nframes, in_b, out_b,
-                                float_frame, detect);
+    const pfa_status st = pfa::run_host_frames(p, reinterpret_cast<const void *const *>(sig_hosts), out_hosts, nframes,
+                                               in_b, out_b, float_frame, detect);
+    return st != PFA_OK ? st : mixed_timeout_check(p);
 }
 
 pfa_status pfa_autofocus_grad(pfa_plan *p, const float *sig_dev, const float *theta_dev, float *dtheta_dev,

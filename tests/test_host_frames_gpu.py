@@ -82,3 +82,17 @@ def test_frames_errors(torch_cuda):
         st = fplan._lib.pfa_form_fixed_host_frames(fplan.handle, engine._frame_ptrs([sig]),
                                                    engine._frame_ptrs([out]), 1)
         assert st == _lib.BAD_CONFIG
+
+
+def test_mixed_host_frames(torch_cuda):
+    """Split-precision plans through the host entry points (both axes on the tensor cores): pipelined
+    frames equal single frames, and the completion-wait status reads clean."""
+    sc = synth.make_scene(2000, 1800, n_targets=8, seed=76, jitter=0.3)
+    tb = geometry.prepare_tables_from_scene(sc)
+    sigs = _frames(torch_cuda, sc, 3, 77)
+    with engine.FloatPlan(2000, 1800, mixed=True) as plan:
+        plan.set_tables(tb)
+        imgs = plan.form_host_frames(sigs)
+        single = [plan.form_host(s) for s in sigs]
+    for k in range(len(sigs)):
+        assert np.array_equal(imgs[k], single[k])
