@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "pfa_internal.h"
 
@@ -406,6 +407,7 @@ struct BfpFft {
         int e_row = 0;
         int done = 0;
         int rbuf = 0;
+        int cur_max = 32768;                    // bound on |re|, |im| of the stage input (CTA-uniform)
         const int lane = tid & 31, warp = tid >> 5;
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
@@ -434,24 +436,35 @@ struct BfpFft {
                 const uint32_t *tws = tw + ((1 << b) - 1);
                 // row max of |re|, |im| as max(largest, -smallest): no |.| per value
                 int hi = 0, lo_ = 0;
+                auto butterflies = [&](auto sat_tag) {
+                    constexpr bool SAT = decltype(sat_tag)::value;
 #pragma unroll
-                for (int v = 0; v < E; ++v) {
-                    if (v & (1 << rb)) continue;
-                    const int v2 = v | (1 << rb);
-                    const int k = tlow | ((v & ((1 << rb) - 1)) << lo);
-                    const uint32_t w = tws[k];
-                    const int wr = lo16(w), wi = hi16(w);
-                    const int br = xr[v2], bi = xi[v2];
-                    const int tr = sat16((wr * br - wi * bi) >> 15);
-                    const int ti = sat16((wr * bi + wi * br) >> 15);
-                    const int ar = xr[v], ai = xi[v];
-                    xr[v] = ar + tr;
-                    xi[v] = ai + ti;
-                    xr[v2] = ar - tr;
-                    xi[v2] = ai - ti;
-                    hi = __vimax3_s32(hi, __vimax3_s32(xr[v], xi[v], xr[v2]), xi[v2]);
-                    lo_ = __vimin3_s32(lo_, __vimin3_s32(xr[v], xi[v], xr[v2]), xi[v2]);
-                }
+                    for (int v = 0; v < E; ++v) {
+                        if (v & (1 << rb)) continue;
+                        const int v2 = v | (1 << rb);
+                        const int k = tlow | ((v & ((1 << rb) - 1)) << lo);
+                        const uint32_t w = tws[k];
+                        const int wr = lo16(w), wi = hi16(w);
+                        const int br = xr[v2], bi = xi[v2];
+                        int tr = (wr * br - wi * bi) >> 15;
+                        int ti = (wr * bi + wi * br) >> 15;
+                        if constexpr (SAT) {
+                            tr = sat16(tr);
+                            ti = sat16(ti);
+                        }
+                        const int ar = xr[v], ai = xi[v];
+                        xr[v] = ar + tr;
+                        xi[v] = ai + ti;
+                        xr[v2] = ar - tr;
+                        xi[v2] = ai - ti;
+                        hi = __vimax3_s32(hi, __vimax3_s32(xr[v], xi[v], xr[v2]), xi[v2]);
+                        lo_ = __vimin3_s32(lo_, __vimin3_s32(xr[v], xi[v], xr[v2]), xi[v2]);
+                    }
+                };
+                // |t| <= |w| |b| / 2^15 + 1 <= 1.4143 cur_max + 1 (|w| <= 32770, |b| <= sqrt(2) cur_max):
+                // with cur_max <= 23000 the twiddle product cannot leave int16, so its saturation is skipped
+                if (cur_max <= 23000) butterflies(std::false_type{});
+                else butterflies(std::true_type{});
                 const unsigned mx = __reduce_max_sync(0xffffffffu, (unsigned)max(hi, -lo_));
                 if (lane == 0) red[rbuf][warp] = (int)mx;
                 __syncthreads();
@@ -479,6 +492,7 @@ struct BfpFft {
                         xi[v] >>= sh;
                     }
                 }
+                cur_max = sh ? (rowmax >> sh) + 1 : rowmax;   // bound on |re|, |im| entering the next stage
                 e_row += sh;
             }
             done = lo + LE;

@@ -19,7 +19,8 @@ Outputs (JSON, a few KB):
                      gen_resample_vectors.gather_cubic and of model_detect_fusion.order_B_fused on
                      seeded operands (``variant_inputs``): the cubic interpolator and the
                      silicon-order detect the engine offers as variants.
-  big_frames.json    (--big) the Centerfield-shaped full frame.
+  big_frames.json    (--big) the Centerfield-shaped full frame and a tiny scene on the largest grid
+                     (16384^2, about 15 minutes of the reference emulator).
 """
 from __future__ import annotations
 
@@ -60,6 +61,11 @@ FLOAT_CASES = [
 
 BIG_CASES = [
     ("centerfield_5634x4319_sinc", "centerfield_5634x4319", 8192, True, True),
+]
+
+# the largest grid the engine accepts (16384^2), on a tiny scene so the reference emulator finishes
+MAX_GRID_CASES = [
+    ("tiny40x48_g16384_sinc", dict(m=40, n=48, n_targets=4, snr_db=20.0, seed=23), 16384, True, True),
 ]
 
 
@@ -156,6 +162,19 @@ def big_cases():
     return out
 
 
+def max_grid_cases():
+    out = {}
+    for name, kw, grid, rs, az in MAX_GRID_CASES:
+        sc = synth.make_scene(**kw)
+        t = time.time()
+        img = refshim.emulator_form_image(sc, grid, rs, az)
+        out[name] = dict(scene=kw, grid=grid, range_sinc=rs, az_sinc=az, input_crc=crc(sc.signal),
+                         image_crc=crc(img.astype("<u2")), image_max=int(img.max()),
+                         seconds=round(time.time() - t, 1))
+        print(name, hex(out[name]["image_crc"]), out[name]["seconds"], "s", flush=True)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--big", action="store_true")
@@ -168,7 +187,9 @@ def main():
         (HERE / "fft_kat.json").write_text(json.dumps(fft_kat(), indent=1))
         (HERE / "variants.json").write_text(json.dumps(variants(), indent=1))
     if a.big or a.only_big:
-        (HERE / "big_frames.json").write_text(json.dumps(dict(env=env, cases=big_cases()), indent=1))
+        cases = big_cases()
+        cases.update(max_grid_cases())
+        (HERE / "big_frames.json").write_text(json.dumps(dict(env=env, cases=cases), indent=1))
 
 
 if __name__ == "__main__":

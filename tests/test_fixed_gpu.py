@@ -200,3 +200,17 @@ def test_silicon_variants_bit_exact(torch_cuda, rmode, amode, order):
         img = plan.form(sc.signal)
     assert np.array_equal(img, ref), f"{(img != ref).sum()} pixels differ"
 
+
+
+def test_largest_grid_matches_reference_crc(torch_cuda):
+    """The largest grid (16384^2: 14-stage BFP FFTs of 1024-thread CTAs) against the reference
+    emulator's CRC on a tiny scene (too large for the oracle in a test)."""
+    c = BIG.get("tiny40x48_g16384_sinc")
+    if c is None:
+        pytest.skip("golden not generated")
+    sc = synth.make_scene(**c["scene"])
+    if _crc(sc.signal) != c["input_crc"]:
+        pytest.skip("synthetic input not bit-identical on this host")
+    tb = geometry.prepare_tables_from_scene(sc)
+    img, *_ = _form(torch_cuda, sc.signal, tb, c["grid"], c["range_sinc"], c["az_sinc"])
+    assert fe.frame_crc(img) == c["image_crc"]
