@@ -520,12 +520,11 @@ __global__ void __launch_bounds__((1 << L) / E) k_fx_pass2_fft(Pass2Args a) {
     using F = BfpFft<L, E>;
     constexpr int N = F::N, T = F::T;
     extern __shared__ __align__(16) unsigned char smem[];
-    // layout: [region A: row u32[m] + src coords f32[m] | exchange buffer] [tw N] [sinc] [red]
+    // layout: [region A: row as int32 I/Q pairs | exchange buffer] [tw N] [sinc] [red]
     const int m = a.m;
-    const size_t rowb = ((size_t)4 * m + 15) & ~(size_t)15;
-    const size_t regA = (max(rowb + (size_t)4 * m, (size_t)4 * (N + N / 32)) + 15) & ~(size_t)15;
-    uint32_t *row = reinterpret_cast<uint32_t *>(smem);
-    float *srcx = reinterpret_cast<float *>(smem + rowb);
+    const size_t rowb = (size_t)32 * ((m + 3) >> 2);
+    const size_t regA = (max(rowb, (size_t)4 * (N + N / 32)) + 15) & ~(size_t)15;
+    int2 *row = reinterpret_cast<int2 *>(smem);
     uint32_t *xbuf = reinterpret_cast<uint32_t *>(smem);
     uint32_t *tw = reinterpret_cast<uint32_t *>(smem + regA);
     int16_t *tab = reinterpret_cast<int16_t *>(smem + regA + 4 * (size_t)N);
@@ -533,22 +532,28 @@ __global__ void __launch_bounds__((1 << L) / E) k_fx_pass2_fft(Pass2Args a) {
 
     const int tid = threadIdx.x;
     const int j = blockIdx.x;                       // range bin (< n)
-    // the p1 row, the twiddles and the sinc table stream in while the source coordinates are computed
+    // the twiddles and the sinc table stream in while the p1 row is unpacked into int32 I/Q pairs (one
+    // 8-byte shared load per sinc tap, no sign extension in the gather)
     {
-        const uint32_t *src = a.p1 + (size_t)j * a.mpad;            // 128-byte aligned rows, mpad >= m
-        for (int c = tid; c < (m + 3) >> 2; c += T) cp_async16(row + 4 * c, src + 4 * c);
         for (int c = tid; c < N / 4; c += T) cp_async16(tw + 4 * c, a.tw + 4 * c);
         if (SINC)
             for (int c = tid; c < 256 * kSincTaps / 8; c += T) cp_async16(tab + 8 * c, a.sinc + 8 * c);
         cp_async_commit();
+        const uint4 *src = reinterpret_cast<const uint4 *>(a.p1 + (size_t)j * a.mpad);   // 128-byte aligned, mpad >= m
+        int4 *dst = reinterpret_cast<int4 *>(row);
+        for (int c = tid; c < (m + 3) >> 2; c += T) {
+            const uint4 v = __ldg(src + c);
+            dst[2 * c] = make_int4(lo16(v.x), hi16(v.x), lo16(v.y), hi16(v.y));
+            dst[2 * c + 1] = make_int4(lo16(v.z), hi16(v.z), lo16(v.w), hi16(v.w));
+        }
     }
-    const float krj = a.krp[j];
-    for (int r = tid; r < m; r += T) srcx[r] = __fmul_rn(krj, a.tan_s[r]);   // KRp[j] * tan_s in float32 (silicon_emulator.py:152)
     cp_async_wait_all();
     __syncthreads();
 
-    const bool asc = srcx[m - 1] >= srcx[0];
-    auto xa = [&](int t) { return (double)(asc ? srcx[t] : srcx[m - 1 - t]); };
+    // source coordinates KRp[j] * tan_s in float32 (silicon_emulator.py:152), from the L1-resident tan_s
+    const float krj = a.krp[j];
+    const bool asc = __fmul_rn(krj, a.tan_s[m - 1]) >= __fmul_rn(krj, a.tan_s[0]);
+    auto xa = [&](int t) { return (double)__fmul_rn(krj, __ldg(a.tan_s + (asc ? t : m - 1 - t))); };
     const double lo_v = xa(0), hi_v = xa(m - 1);
     const double inv_span = (double)(m - 1) / (hi_v - lo_v);
     const int hr = a.hamr[j];
@@ -693,8 +698,7 @@ struct FixedLaunch {
     static constexpr int T = N / E;
 
     static size_t pass2_smem(int m, bool sinc) {
-        const size_t rowb = ((size_t)4 * m + 15) & ~(size_t)15;
-        size_t regA = rowb + (size_t)4 * m;
+        size_t regA = (size_t)32 * ((m + 3) >> 2);
         const size_t xb = (size_t)4 * (N + N / 32);
         if (xb > regA) regA = xb;
         regA = (regA + 15) & ~(size_t)15;
