@@ -16,8 +16,9 @@ from .engine import FloatPlan
 
 class BatchFormer:
     def __init__(self, scenes, range_sinc=False, az_sinc=False, streams=4, tiles=None, af_iters=0,
-                 af_step=0.3, device=0):
-        """scenes: list of (tables, signal) with signal an (m, n) complex64 CUDA tensor."""
+                 af_step=0.3, device=0, mixed=False):
+        """scenes: list of (tables, signal) with signal an (m, n) complex64 CUDA tensor.  ``mixed``: form
+        the final images with the split-precision tensor-core FFTs (the autofocus gradients stay FP32)."""
         import torch
         self.torch = torch
         self.n = len(scenes)
@@ -27,7 +28,7 @@ class BatchFormer:
         for i, (tb, sig) in enumerate(scenes):
             m, n = tuple(sig.shape)
             tile = tiles[i] if tiles is not None else (16, 16)
-            p = FloatPlan(m, n, range_sinc, az_sinc, device=device, tile=tile)
+            p = FloatPlan(m, n, range_sinc, az_sinc, mixed=mixed, device=device, tile=tile)
             p.set_tables(tb)
             self.plans.append(p)
         dev = self.signals[0].device

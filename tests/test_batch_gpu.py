@@ -87,3 +87,26 @@ def test_batch_with_autofocus_iterations(torch_cuda):
     for a, b in zip(th_eager, bf.theta):
         assert torch.allclose(a, b, atol=1e-4)
     bf.close()
+
+
+def test_mixed_batch_graph(torch_cuda):
+    """Mixed-precision images in the multi-stream graph (scenes with 2048/4096-point lines on the tensor
+    cores next to FP32 ones): the graph replay equals the eager run and each image is within the mixed
+    error budget of the FP32 image."""
+    torch = torch_cuda
+    scenes = _scenes(torch, [(2000, 1500), (700, 3000), (1200, 600)], 90)
+    bf = batch.BatchFormer(scenes, streams=3, mixed=True, af_iters=2)
+    bf.run_eager()
+    torch.cuda.synchronize()
+    eager = [im.clone() for im in bf.images]
+    bf.replay()
+    torch.cuda.synchronize()
+    for a, b in zip(eager, bf.images):
+        assert fp.rel_l2(b.cpu().numpy(), a.cpu().numpy()) <= 1e-4
+    ref = batch.BatchFormer(scenes, streams=1, af_iters=2)
+    ref.run_eager()
+    torch.cuda.synchronize()
+    for a, b in zip(ref.images, bf.images):
+        assert fp.rel_l2(b.cpu().numpy(), a.cpu().numpy()) <= 1e-4
+    ref.close()
+    bf.close()
