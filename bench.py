@@ -201,6 +201,21 @@ def measure_modes(a, local):
         out[name] = {"workload": "ndsu_8167x8192 -> 8192^2", "ms_per_frame": round(ms, 4),
                      "stages_ms": {k: round(v, 4) for k, v in st.items()},
                      "frame_bytes": fb, "frame_frac_of_hbm": round(fb / (ms * 1e-3) / 1e9 / _peaks()[0], 4)}
+        if name == "float_fp32_lerp":
+            # end to end through the pipelined host-buffer entry point (pinned host in/out, PCIe included)
+            sig_h = torch.empty(tuple(sig.shape), dtype=torch.complex64).pin_memory()
+            sig_h.copy_(sig)
+            outs_h = [torch.empty((8192, 8192), dtype=torch.float32).pin_memory() for _ in range(2)]
+            with engine.FloatPlan(8167, 8192, device=local) as hp:
+                hp.set_tables(tables)
+                frames = [sig_h.numpy()] * 4
+                outs = [outs_h[k & 1].numpy() for k in range(4)]
+                hp.form_host_frames(frames[:2], outs[:2])
+                t0 = time.perf_counter()
+                hp.form_host_frames(frames, outs)
+                out[name]["e2e_ms_per_frame"] = round((time.perf_counter() - t0) * 1000.0 / 4, 4)
+                out[name]["e2e_bytes_per_frame"] = {"h2d": int(sig_h.numel() * 8), "d2h": 8192 * 8192 * 4}
+            del sig_h, outs_h
         if not mixed:
             ref_c[rs] = (cz, ms)
         else:
