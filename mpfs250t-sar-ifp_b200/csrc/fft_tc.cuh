@@ -8,7 +8,8 @@
 //   X[k2 + N2 k1] = sum_n1 F_128[k1][n1] T[n1][k2]                       (stage 2: A = F_128 in TMEM,
 //                                                                          B = T in shared memory)
 // Every real product P Q runs as Ph Qh + Ph Ql + Pl Qh with fp16 hi/lo parts (v = hi + lo, 22
-// significant bits) and fp32 accumulation; complex products are spelled out in real parts.  The line
+// significant bits) and fp32 accumulation; complex products are spelled out in real parts, the
+// subtracted ones with the B operand negated by the instruction descriptor.  The line
 // is scaled by a power of two s1 so that its largest component lies in [2^14, 2^15) (fp16 range with
 // headroom); after stage 1 the scale becomes s1 / N2, which bounds |T| by the same range.
 //
@@ -18,12 +19,12 @@
 // TMEM (512 columns, one CTA per SM):
 //   [0, 256)                 F_128 as the stage-2 A operand: Frh, Frl, Fih, Fil (64 columns each,
 //                            two fp16 of consecutive n1 per 32-bit column)
-//   [256, 256 + 2 N2)        stage-1 A operand: Arh, Arl, Aih, Ail (N2/2 columns each)
-//   [256 + 2 N2, 256 + 4 N2) stage-1 accumulators D1r, D1i
-//   [256, 256 + 3 N2)        stage-2 accumulators P = Fr.Tr, Q = Fi.Ti, I = Fr.Ti + Fi.Tr (reuse the
-//                            dead stage-1 columns; Re X = P - Q, Im X = I, so no operand is negated)
-// Shared memory: F_N2 image (6 arrays: Frh, Frl, Fih, Fil, -Fih, -Fil; MN-major N2 x N2) and the
-// stage-2 B operand (4 arrays Trh, Trl, Tih, Til; MN-major, K = 128 rows n1, N = N2 columns k2).
+//   [256, 256 + 2 N2)        stage-1 A operand: Arh, Arl, Aih, Ail (N2/2 columns each); free while
+//                            stage 2 runs, so the next line's input can be written meanwhile
+//   [256 + 2 N2, 256 + 4 N2) accumulators Re, Im: stage 1's D1, then stage 2's X (the products with
+//                            a minus sign negate their B operand through the instruction descriptor)
+// Shared memory: F_N2 image (4 arrays: Frh, Frl, Fih, Fil; MN-major N2 x N2) and the stage-2 B operand
+// (4 arrays Trh, Trl, Tih, Til; MN-major, K = 128 rows n1, N = N2 columns k2).
 #pragma once
 
 #include <cuda_fp16.h>
@@ -43,10 +44,9 @@ struct Geo {
     static_assert(N2 == 16 || N2 == 32 || N2 == 64, "tensor-core FFT lines are 2048, 4096 or 8192 points");
     static constexpr int NG = N2 / 16;
     static constexpr int THREADS = 128 * NG;
-    static constexpr uint32_t COL_F = 0, COL_A = 256, COL_D1 = 256 + 2 * N2, TMEM_COLS = 512;
-    static constexpr uint32_t COL_P = 256, COL_Q = 256 + N2, COL_I = 256 + 2 * N2;
+    static constexpr uint32_t COL_F = 0, COL_A = 256, COL_D = 256 + 2 * N2, TMEM_COLS = 512;
     static constexpr uint32_t FN2_ARR = (uint32_t)N2 * N2 * 2;
-    static constexpr uint32_t FN2_BYTES = 6 * FN2_ARR;
+    static constexpr uint32_t FN2_BYTES = 4 * FN2_ARR;
     static constexpr uint32_t B2_ARR = 128u * N2 * 2;
     static constexpr uint32_t B2_BYTES = 4 * B2_ARR;           // = 8 N: also holds one complex line
 };
@@ -140,17 +140,19 @@ struct TcFft {
     // Stage 1 (one thread): D1r = Ar Fr - Ai Fi, D1i = Ar Fi + Ai Fr, each real product split three ways.
     __device__ static void issue_stage1(uint32_t tm, uint32_t fn2) {
         constexpr uint32_t idesc = tc::idesc_f16(128, N2, false, true);
-        // {A array (Arh, Arl, Aih, Ail), F_N2 array (Frh, Frl, Fih, Fil, -Fih, -Fil), accumulator (re, im)}
-        constexpr int8_t terms[12][3] = {{0, 0, 0}, {0, 1, 0}, {1, 0, 0}, {2, 4, 0}, {2, 5, 0}, {3, 4, 0},
-                                         {0, 2, 1}, {0, 3, 1}, {1, 2, 1}, {2, 0, 1}, {2, 1, 1}, {3, 0, 1}};
+        constexpr uint32_t idesc_neg = tc::idesc_f16(128, N2, false, true, false, true);   // -B
+        // {A array (Arh, Arl, Aih, Ail), F_N2 array (Frh, Frl, Fih, Fil), accumulator (re, im), negate B}
+        constexpr int8_t terms[12][4] = {{0, 0, 0, 0}, {0, 1, 0, 0}, {1, 0, 0, 0}, {2, 2, 0, 1}, {2, 3, 0, 1},
+                                         {3, 2, 0, 1}, {0, 2, 1, 0}, {0, 3, 1, 0}, {1, 2, 1, 0}, {2, 0, 1, 0},
+                                         {2, 1, 1, 0}, {3, 0, 1, 0}};
 #pragma unroll
         for (int t = 0; t < 12; ++t) {
 #pragma unroll
             for (int s = 0; s < N2 / 16; ++s) {
                 const uint32_t a = tm + G::COL_A + terms[t][0] * (N2 / 2) + 8 * s;
                 const uint64_t b = tc::smem_desc(fn2 + terms[t][1] * G::FN2_ARR + s * 2 * N2 * 16, N2 * 16, 128);
-                const uint32_t d = tm + G::COL_D1 + terms[t][2] * N2;
-                tc::mma_ts(d, a, b, idesc, !((t == 0 || t == 6) && s == 0));
+                const uint32_t d = tm + G::COL_D + terms[t][2] * N2;
+                tc::mma_ts(d, a, b, terms[t][3] ? idesc_neg : idesc, !((t == 0 || t == 6) && s == 0));
             }
         }
     }
@@ -166,8 +168,8 @@ struct TcFft {
     __device__ static void epilogue1(uint32_t tm, unsigned char *b2, const float2 (&tw)[16], int q, int g, int lane) {
         const int n1 = 32 * q + lane;
         uint32_t re[16], im[16];
-        tc::tmem_ld16(lane_base(tm, q) + G::COL_D1 + 16 * g, re);
-        tc::tmem_ld16(lane_base(tm, q) + G::COL_D1 + N2 + 16 * g, im);
+        tc::tmem_ld16(lane_base(tm, q) + G::COL_D + 16 * g, re);
+        tc::tmem_ld16(lane_base(tm, q) + G::COL_D + N2 + 16 * g, im);
         tc::tmem_wait_ld();
         constexpr float inv = 1.0f / (float)N2;
 #pragma unroll
@@ -197,33 +199,35 @@ struct TcFft {
         }
     }
 
-    // Stage 2 (one thread): P = Fr Tr, Q = Fi Ti, I = Fr Ti + Fi Tr (each real product split three ways).
+    // Stage 2 (one thread): Re = Fr Tr - Fi Ti, Im = Fr Ti + Fi Tr (each real product split three ways),
+    // into the accumulator columns stage 1 used (read by epilogue 1 before this is issued).
     __device__ static void issue_stage2(uint32_t tm, uint32_t b2) {
         constexpr uint32_t idesc = tc::idesc_f16(128, N2, false, true);
-        // {F_128 array (Frh, Frl, Fih, Fil), T array (Trh, Trl, Tih, Til), accumulator (P, Q, I)}
-        constexpr int8_t terms[12][3] = {{0, 0, 0}, {0, 1, 0}, {1, 0, 0}, {2, 2, 1}, {2, 3, 1}, {3, 2, 1},
-                                         {0, 2, 2}, {0, 3, 2}, {1, 2, 2}, {2, 0, 2}, {2, 1, 2}, {3, 0, 2}};
+        constexpr uint32_t idesc_neg = tc::idesc_f16(128, N2, false, true, false, true);   // -B
+        // {F_128 array (Frh, Frl, Fih, Fil), T array (Trh, Trl, Tih, Til), accumulator (re, im), negate B}
+        constexpr int8_t terms[12][4] = {{0, 0, 0, 0}, {0, 1, 0, 0}, {1, 0, 0, 0}, {2, 2, 0, 1}, {2, 3, 0, 1},
+                                         {3, 2, 0, 1}, {0, 2, 1, 0}, {0, 3, 1, 0}, {1, 2, 1, 0}, {2, 0, 1, 0},
+                                         {2, 1, 1, 0}, {3, 0, 1, 0}};
 #pragma unroll
         for (int t = 0; t < 12; ++t) {
 #pragma unroll
             for (int s = 0; s < 8; ++s) {
                 const uint32_t a = tm + G::COL_F + terms[t][0] * 64 + 8 * s;
                 const uint64_t b = tc::smem_desc(b2 + terms[t][1] * G::B2_ARR + s * 2 * N2 * 16, N2 * 16, 128);
-                const uint32_t d = tm + G::COL_P + terms[t][2] * N2;
-                tc::mma_ts(d, a, b, idesc, !((t % 3) == 0 && (t == 0 || t == 3 || t == 6) && s == 0));
+                const uint32_t d = tm + G::COL_D + terms[t][2] * N2;
+                tc::mma_ts(d, a, b, terms[t][3] ? idesc_neg : idesc, !((t == 0 || t == 6) && s == 0));
             }
         }
     }
 
     // Stage-2 result of lane k1 = 32 q + lane: y[c] = X[16 g + c + N2 k1] * s1 / N2 (unscaled by the caller).
     __device__ static void get_output(float2 (&y)[16], uint32_t tm, int q, int g) {
-        uint32_t p[16], qq[16], ii[16];
-        tc::tmem_ld16(lane_base(tm, q) + G::COL_P + 16 * g, p);
-        tc::tmem_ld16(lane_base(tm, q) + G::COL_Q + 16 * g, qq);
-        tc::tmem_ld16(lane_base(tm, q) + G::COL_I + 16 * g, ii);
+        uint32_t re[16], im[16];
+        tc::tmem_ld16(lane_base(tm, q) + G::COL_D + 16 * g, re);
+        tc::tmem_ld16(lane_base(tm, q) + G::COL_D + N2 + 16 * g, im);
         tc::tmem_wait_ld();
 #pragma unroll
-        for (int c = 0; c < 16; ++c) y[c] = make_float2(__uint_as_float(p[c]) - __uint_as_float(qq[c]), __uint_as_float(ii[c]));
+        for (int c = 0; c < 16; ++c) y[c] = make_float2(__uint_as_float(re[c]), __uint_as_float(im[c]));
     }
 };
 

@@ -128,29 +128,31 @@ __global__ void __launch_bounds__(Geo<L>::THREADS, 1) k_mx_fft2(MxFft2Args a) {
     const int ln = 32 * q + lane;                            // TMEM lane: n1 on input, k1 on output
     float2 twr[16];
     F::twiddles(twr, a.tw, ln, g);
+    // Software pipeline over this CTA's lines: while the tensor core runs stage 1 of line r the CUDA
+    // cores detect and store line r - step; while it runs stage 2 of line r they scale, split and stage
+    // line r + step into the (then free) stage-1 operand columns.
     float2 xn[16];
     auto load_row = [&](int r) {
-        const float2 *row = a.y1t + (size_t)r * a.npad;
+        // the cross-FFT rows are already conjugated for the inverse (pass 2 conjugates its input)
 #pragma unroll
         for (int c = 0; c < 16; ++c) {
             const int j = ln + 128 * (16 * g + c);            // range bins j >= n are the zero pad
-            xn[c] = j < a.n ? __ldcs(row + j) : make_float2(0.f, 0.f);
+            xn[c] = j < a.n ? __ldcs(a.y1t + (size_t)r * a.npad + j) : make_float2(0.f, 0.f);
         }
     };
-    if ((int)blockIdx.x < a.rows) load_row(blockIdx.x);
-    for (int r = blockIdx.x; r < a.rows; r += gridDim.x) {
-        // the cross-FFT rows are already conjugated for the inverse (pass 2 conjugates its input)
-        float2 x[16];
+    // scale and stage the line held in xn into the stage-1 operand; returns its scale
+    auto stage_input = [&]() {
         float mx = 0.f;
 #pragma unroll
-        for (int c = 0; c < 16; ++c) {
-            x[c] = xn[c];
-            mx = fmaxf(mx, fmaxf(fabsf(x[c].x), fabsf(x[c].y)));
-        }
-        if (r + (int)gridDim.x < a.rows) load_row(r + gridDim.x);   // next line in flight meanwhile
+        for (int c = 0; c < 16; ++c) mx = fmaxf(mx, fmaxf(fabsf(xn[c].x), fabsf(xn[c].y)));
         const float s1 = F::line_scale(mx, red, warp, lane);
-        float2 y[16];
-        ok = tc_line<L>(x, s1, y, tm, fn2_s, b2, b2_s, twr, &bar, phase, ok, tid, q, g, lane);
+        if (ok) {
+            tc::fence_after_sync();
+            F::put_input(xn, s1, tm, q, g);
+        }
+        return s1;
+    };
+    auto emit = [&](const float2 (&y)[16], float s1, int r) {
         const float sc = a.scale * ((float)N2 / s1);
         const float cs = a.inverse ? -sc : sc;                // inverse: conj(FFT(conj(x)))
         const int v0 = N2 * ln + 16 * g;                      // first output column of this thread
@@ -186,7 +188,63 @@ __global__ void __launch_bounds__(Geo<L>::THREADS, 1) k_mx_fft2(MxFft2Args a) {
             float4 *dst = reinterpret_cast<float4 *>(static_cast<float *>(a.out) + (size_t)r * N);
             for (int ch = tid; ch < N / 4; ch += T) __stcs(dst + ch, stg[tcfft::swz_chunk<ilog2c(N2 / 4)>(ch)]);
         }
+    };
+    const int step = gridDim.x;
+    int r = blockIdx.x;                                       // < rows: the grid is min(rows, SMs)
+    load_row(r);
+    float s_cur = stage_input();
+    if (r + step < a.rows) load_row(r + step);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0 && ok) {
+        tc::fence_after_sync();
+        F::issue_stage1(tm, fn2_s);
+        tc::commit(&bar);
     }
+    float2 yprev[16];
+    float s_prev = 1.f;
+    int r_prev = -1;
+    for (; r < a.rows; r += step) {
+        const int rn = r + step;
+        if (r_prev >= 0) emit(yprev, s_prev, r_prev);         // overlaps stage 1 of line r
+        ok = cta_wait(&bar, phase, ok);
+        phase ^= 1u;
+        tc::fence_after_sync();
+        if (ok) F::epilogue1(tm, b2, twr, q, g, lane);
+        tc::fence_smem_to_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid == 0 && ok) {
+            tc::fence_after_sync();
+            F::issue_stage2(tm, b2_s);
+            tc::commit(&bar);
+        }
+        float s_next = 1.f;
+        if (rn < a.rows) {                                    // overlaps stage 2 of line r
+            s_next = stage_input();
+            if (rn + step < a.rows) load_row(rn + step);
+        }
+        ok = cta_wait(&bar, phase, ok);
+        phase ^= 1u;
+        tc::fence_after_sync();
+        if (ok) {
+            F::get_output(yprev, tm, q, g);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 16; ++c) yprev[c] = make_float2(0.f, 0.f);
+        }
+        s_prev = s_cur;
+        r_prev = r;
+        s_cur = s_next;
+        tc::fence_before_sync();
+        __syncthreads();
+        if (rn < a.rows && tid == 0 && ok) {
+            tc::fence_after_sync();
+            F::issue_stage1(tm, fn2_s);
+            tc::commit(&bar);
+        }
+    }
+    if (r_prev >= 0) emit(yprev, s_prev, r_prev);
     if (!ok && tid == 0) atomicExch(a.err, 1);
     tc::fence_before_sync();
     __syncthreads();
@@ -405,9 +463,9 @@ void split_host(double v, uint16_t &hi, uint16_t &lo) {
     lo = __half_raw(l).x;
 }
 
-// F_N2 shared-memory image: arrays Frh, Frl, Fih, Fil, -Fih, -Fil, element (n2, k2) MN-major
+// F_N2 shared-memory image: arrays Frh, Frl, Fih, Fil, element (n2, k2) MN-major
 std::vector<uint16_t> fn2_image(int N2) {
-    std::vector<uint16_t> img(6 * (size_t)N2 * N2);
+    std::vector<uint16_t> img(4 * (size_t)N2 * N2);
     const size_t arr = (size_t)N2 * N2;
     for (int a = 0; a < N2; ++a)
         for (int b = 0; b < N2; ++b) {
@@ -420,8 +478,6 @@ std::vector<uint16_t> fn2_image(int N2) {
             img[1 * arr + o] = rl;
             img[2 * arr + o] = ih;
             img[3 * arr + o] = il;
-            img[4 * arr + o] = ih ^ 0x8000u;                 // exact fp16 negation
-            img[5 * arr + o] = il ^ 0x8000u;
         }
     return img;
 }
