@@ -43,51 +43,6 @@ __device__ __forceinline__ bool cta_wait(uint64_t *bar, uint32_t parity, bool ok
     return __syncthreads_and(mine) != 0;
 }
 
-// One line through both tensor-core stages: x (16 values per thread, scaled by s1 inside) -> y.
-// Returns false (and y = 0) once a completion wait has timed out.
-template <int L>
-__device__ __forceinline__ bool tc_line(const float2 (&x)[16], float s1, float2 (&y)[16], uint32_t tm,
-                                        uint32_t fn2_s, unsigned char *b2, uint32_t b2_s, const float2 (&tw)[16],
-                                        uint64_t *bar, uint32_t &phase, bool ok, int tid, int q, int g, int lane) {
-    using F = TcFft<L>;
-    if (ok) {
-        tc::fence_after_sync();
-        F::put_input(x, s1, tm, q, g);
-        tc::fence_before_sync();
-        __syncthreads();
-        if (tid == 0) {
-            tc::fence_after_sync();
-            F::issue_stage1(tm, fn2_s);
-            tc::commit(bar);
-        }
-        ok = cta_wait(bar, phase, ok);
-        phase ^= 1u;
-        tc::fence_after_sync();
-    }
-    if (ok) {
-        F::epilogue1(tm, b2, tw, q, g, lane);
-        tc::fence_smem_to_async();
-        tc::fence_before_sync();
-        __syncthreads();
-        if (tid == 0) {
-            tc::fence_after_sync();
-            F::issue_stage2(tm, b2_s);
-            tc::commit(bar);
-        }
-        ok = cta_wait(bar, phase, ok);
-        phase ^= 1u;
-        tc::fence_after_sync();
-    }
-    if (ok) {
-        F::get_output(y, tm, q, g);
-    } else {
-#pragma unroll
-        for (int c = 0; c < 16; ++c) y[c] = make_float2(0.f, 0.f);
-    }
-    tc::fence_before_sync();
-    return ok;
-}
-
 // ------------------------------------------------------------------------------------------ range FFT
 struct MxFft2Args {
     const float2 *y1t;
@@ -310,10 +265,10 @@ __global__ void __cluster_dims__(kMxCT, 1, 1) __launch_bounds__(Geo<L>::THREADS,
         for (int c = tid; c < ((m + 1) >> 1); c += T) cp_async16(row + 2 * c, src + 2 * c);
         cp_async_commit();
     };
-    fetch_row(cid);
-    for (int grp = cid; grp < a.ngroups; grp += ncl) {
-        const int j = grp * kMxCT + rank;                     // range bin of this CTA
-        float2 x[16];
+    // The pass-2 line of group grp (this CTA's range bin): gather, window, centring sign, conj for the
+    // inverse; returns the line's max |component|.  Reads the p1 row fetched into shared memory.
+    auto gather_line = [&](int grp, float2 (&x)[16]) {
+        const int j = grp * kMxCT + rank;
         float mx = 0.f;
         if (j < a.n) {
             const double krj = a.kr_grid[j];
@@ -373,11 +328,23 @@ __global__ void __cluster_dims__(kMxCT, 1, 1) __launch_bounds__(Geo<L>::THREADS,
 #pragma unroll
             for (int c = 0; c < 16; ++c) x[c] = make_float2(0.f, 0.f);
         }
+        return mx;
+    };
+    // gather line grp, prefetch the row of the line after it, stage it into the stage-1 operand
+    auto stage_line = [&](int grp) {
+        float2 x[16];
+        const float mx = gather_line(grp, x);
         const float s1 = F::line_scale(mx, red, warp, lane);   // its barriers end this line's gather
         fetch_row(grp + ncl);
-        float2 y[16];
-        ok = tc_line<L>(x, s1, y, tm, fn2_s, b2, b2_s, twr, &bar, phase, ok, tid, q, g, lane);
-        // this CTA's line in natural frequency order (stays conjugated for the inverse) -> exchange buffer
+        if (ok) {
+            tc::fence_after_sync();
+            F::put_input(x, s1, tm, q, g);
+        }
+        return s1;
+    };
+    // line grp in natural frequency order (stays conjugated for the inverse) -> exchange buffer, then
+    // corner turn #2: this CTA writes cross bins [rank N/8, (rank+1) N/8) of the cluster's 8 range bins
+    auto exchange = [&](const float2 (&y)[16], float s1, int grp) {
         const float sc = (float)N2 / s1;
         const int v0 = N2 * ln + 16 * g;
         float4 *xch = reinterpret_cast<float4 *>(b2);
@@ -386,7 +353,6 @@ __global__ void __cluster_dims__(kMxCT, 1, 1) __launch_bounds__(Geo<L>::THREADS,
             xch[tcfft::swz_chunk<ilog2c(N2 / 2)>((v0 >> 1) + c)] =
                 make_float4(y[2 * c].x * sc, y[2 * c].y * sc, y[2 * c + 1].x * sc, y[2 * c + 1].y * sc);
         cluster.sync();
-        // corner turn #2: this CTA writes cross bins [rank N/8, (rank+1) N/8) of the cluster's 8 range bins
 #pragma unroll 4
         for (int s2 = 0; s2 < N / T; ++s2) {
             const int item = tid + T * s2;
@@ -397,7 +363,60 @@ __global__ void __cluster_dims__(kMxCT, 1, 1) __launch_bounds__(Geo<L>::THREADS,
             a.y1t[(size_t)k * a.npad + grp * kMxCT + r8] = remote[pos];
         }
         cluster.sync();                                       // the peers are done with this buffer
+    };
+    // Software pipeline over the cluster's groups (every CTA of a cluster runs the same groups, so the
+    // cluster barriers stay matched): the previous line's exchange runs while the tensor core computes
+    // stage 1 of this line, the next line's gather and staging while it computes stage 2.
+    fetch_row(cid);
+    int grp = cid;                                            // < ngroups: the grid has at most ngroups clusters
+    float s_cur = stage_line(grp);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0 && ok) {
+        tc::fence_after_sync();
+        F::issue_stage1(tm, fn2_s);
+        tc::commit(&bar);
     }
+    float2 yprev[16];
+    float s_prev = 1.f;
+    int grp_prev = -1;
+    for (; grp < a.ngroups; grp += ncl) {
+        const int gn = grp + ncl;
+        if (grp_prev >= 0) exchange(yprev, s_prev, grp_prev); // overlaps stage 1 of this line
+        ok = cta_wait(&bar, phase, ok);
+        phase ^= 1u;
+        tc::fence_after_sync();
+        if (ok) F::epilogue1(tm, b2, twr, q, g, lane);
+        tc::fence_smem_to_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid == 0 && ok) {
+            tc::fence_after_sync();
+            F::issue_stage2(tm, b2_s);
+            tc::commit(&bar);
+        }
+        const float s_next = gn < a.ngroups ? stage_line(gn) : 1.f;   // overlaps stage 2 of this line
+        ok = cta_wait(&bar, phase, ok);
+        phase ^= 1u;
+        tc::fence_after_sync();
+        if (ok) {
+            F::get_output(yprev, tm, q, g);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 16; ++c) yprev[c] = make_float2(0.f, 0.f);
+        }
+        s_prev = s_cur;
+        grp_prev = grp;
+        s_cur = s_next;
+        tc::fence_before_sync();
+        __syncthreads();
+        if (gn < a.ngroups && tid == 0 && ok) {
+            tc::fence_after_sync();
+            F::issue_stage1(tm, fn2_s);
+            tc::commit(&bar);
+        }
+    }
+    if (grp_prev >= 0) exchange(yprev, s_prev, grp_prev);
     if (!ok && tid == 0) atomicExch(a.err, 1);
     tc::fence_before_sync();
     __syncthreads();
