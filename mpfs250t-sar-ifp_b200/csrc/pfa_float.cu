@@ -35,8 +35,12 @@ template <int L, int E>
 using F32Fft = StockhamFft<L, E>;
 
 // ------------------------------------------------------------------------------------------ K1f
-constexpr int F1_SLOTS = 32, F1_WARPS = 8, F1_WMAX = 256;
-// range bins per CTA: the sinc variant takes a narrower tile so three CTAs (with the 32 KB table) fit an SM
+// Each warp owns a double-buffered window of its pulse's samples: the window of the next pulse streams
+// in (cp.async) while the current one is gathered.  The KR grid lies inside every pulse's own span, so
+// F1_BINS consecutive bins cover at most F1_BINS + 1 source intervals; a wider window (not produced by
+// prepare_tables) falls back to gathering from global memory.
+constexpr int F1_SLOTS = 32, F1_WARPS = 8, F1_WMAX = 144;
+// range bins per CTA: the sinc variant takes a narrower tile so three CTAs (with the 36 KB table) fit an SM
 constexpr int f1_bins(bool sinc) { return sinc ? 64 : 128; }
 
 struct FPass1Args {
@@ -49,17 +53,27 @@ struct FPass1Args {
     int m, n, mpad;
 };
 
+// per-slot pulse constants, computed once per CTA
+struct F1Pulse {
+    double f0, df, sc, kfirst, klast, inv_dk;
+    float2 rot;
+    int i;          // source pulse, -1 for a slot past the last pulse
+    int asc;
+};
+
 constexpr size_t f1_smem(bool sinc) {
-    return (size_t)f1_bins(sinc) * (F1_SLOTS + 1) * 8 + (size_t)F1_WARPS * F1_WMAX * 8 + (sinc ? kTabFloats * 4 : 0);
+    return (size_t)f1_bins(sinc) * (F1_SLOTS + 1) * 8 + (size_t)F1_WARPS * 2 * F1_WMAX * 8 + (sinc ? kTabFloats * 4 : 0);
 }
 
 template <bool SINC>
-__global__ void __launch_bounds__(256) k_fl_pass1(FPass1Args a) {
+__global__ void __launch_bounds__(256, SINC ? 3 : 4) k_fl_pass1(FPass1Args a) {
     extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int F1_BINS = f1_bins(SINC), TB = F1_BINS / 32, SPW = F1_SLOTS / F1_WARPS;
+    constexpr size_t TILE_BYTES = (size_t)F1_BINS * (F1_SLOTS + 1) * 8;
     float2(*tile)[F1_SLOTS + 1] = reinterpret_cast<float2(*)[F1_SLOTS + 1]>(smem);
-    constexpr int F1_BINS = f1_bins(SINC);
-    float2(*win)[F1_WMAX] = reinterpret_cast<float2(*)[F1_WMAX]>(smem + (size_t)F1_BINS * (F1_SLOTS + 1) * 8);
-    float *tab = reinterpret_cast<float *>(smem + (size_t)F1_BINS * (F1_SLOTS + 1) * 8 + (size_t)F1_WARPS * F1_WMAX * 8);
+    float2(*win)[2][F1_WMAX] = reinterpret_cast<float2(*)[2][F1_WMAX]>(smem + TILE_BYTES);
+    float *tab = reinterpret_cast<float *>(smem + TILE_BYTES + (size_t)F1_WARPS * 2 * F1_WMAX * 8);
+    __shared__ F1Pulse prm[F1_SLOTS];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r0 = blockIdx.x * F1_SLOTS, j0 = blockIdx.y * F1_BINS;
     const int n = a.n;
@@ -69,85 +83,132 @@ __global__ void __launch_bounds__(256) k_fl_pass1(FPass1Args a) {
 #pragma unroll
         for (int i = 0; i < kTabFloats / 4 / 256; ++i) dst[tid + 256 * i] = __ldg(src + tid + 256 * i);
     }
-    __syncthreads();
-    for (int s = 0; s < F1_SLOTS / F1_WARPS; ++s) {
-        const int slot = warp + F1_WARPS * s;
-        const int r = r0 + slot;
-        if (r >= a.m) {
-            for (int t = lane; t < F1_BINS; t += 32) tile[t][slot] = make_float2(0.f, 0.f);
-            continue;
-        }
-        const int i = a.order[r];
-        const double f0 = a.f0[i], df = a.df[i], pri = a.pr[i], sc = 2.0 * pri / kC;
-        // kr[i, k] = (2 freq[i, k] / c) pr[i] (form_image_pfa.py:176-187).  The end points are evaluated
-        // with the reference's exact IEEE operations (KR's first and last samples coincide with some
-        // pulse's end points, where np.interp returns the end sample); interior samples use the affine
-        // model freq = f0 + k df.
-        const double kfirst = __dmul_rn(__ddiv_rn(__dmul_rn(2.0, f0), kC), pri);
-        const double klast = __dmul_rn(__ddiv_rn(__dmul_rn(2.0, a.flast[i]), kC), pri);
-        auto kr = [&](int k) { return k == 0 ? kfirst : (k == n - 1 ? klast : sc * (f0 + (double)k * df)); };
-        const bool asc = kr(n - 1) >= kr(0);
-        auto xa = [&](int t) { return asc ? kr(t) : kr(n - 1 - t); };
-        const double xa0 = xa(0), xa1 = xa(n - 1);
-        const double inv_dk = 1.0 / fabs(sc * df);       // the source axis is affine in the sample index
-        int jj[F1_BINS / 32];
-        Frac fr[F1_BINS / 32];
-        int lo_i = 1 << 30, hi_i = -1;
-#pragma unroll
-        for (int t = 0; t < F1_BINS / 32; ++t) {
-            const int j = j0 + lane + 32 * t;
-            jj[t] = -1;
-            fr[t] = Frac{0.f, 0, 0};
-            if (j < n) {
-                const double q = a.kr_grid[j];
-                int ja = -1;
-                if (q >= xa0 && q <= xa1) {
-                    // closed-form bracket on the affine axis; the end points are exact
-                    const double pos = (q - xa0) * inv_dk;
-                    ja = isfinite(pos) ? min(max((int)floor(pos), 0), n - 2) : 0;
-                    const double fd = (q - xa(ja)) * inv_dk;
-                    fr[t].f = (float)fd;
-                    fr[t].ph = sinc_phase(fd);
-                }
-                if (ja >= 0) {
-                    // natural-order index of the lower sample and the weight toward the upper one
-                    int lowi;
-                    if (asc) { lowi = ja; } else { lowi = n - 2 - ja; mirror_frac(fr[t]); }
-                    jj[t] = lowi;
-                    lo_i = min(lo_i, lowi);
-                    hi_i = max(hi_i, lowi);
-                }
+    if (tid < F1_SLOTS) {
+        F1Pulse p{};
+        p.i = -1;
+        p.rot = make_float2(1.f, 0.f);
+        const int r = r0 + tid;
+        if (r < a.m) {
+            const int i = a.order[r];
+            const double f0 = a.f0[i], df = a.df[i], pri = a.pr[i];
+            p.i = i;
+            p.f0 = f0;
+            p.df = df;
+            p.sc = 2.0 * pri / kC;
+            // kr[i, k] = (2 freq[i, k] / c) pr[i] (form_image_pfa.py:176-187).  The end points are evaluated
+            // with the reference's exact IEEE operations (KR's first and last samples coincide with some
+            // pulse's end points, where np.interp returns the end sample); interior samples use the affine
+            // model freq = f0 + k df.
+            p.kfirst = __dmul_rn(__ddiv_rn(__dmul_rn(2.0, f0), kC), pri);
+            p.klast = __dmul_rn(__ddiv_rn(__dmul_rn(2.0, a.flast[i]), kC), pri);
+            p.inv_dk = 1.0 / fabs(p.sc * df);               // the source axis is affine in the sample index
+            // the phase correction commutes with the (linear, per-pulse) interpolation: rotate the output
+            if (a.theta) {
+                float sn, cs;
+                sincosf(a.theta[i], &sn, &cs);
+                p.rot = make_float2(cs, -sn);
             }
         }
-        lo_i = __reduce_min_sync(0xffffffffu, lo_i);
-        hi_i = __reduce_max_sync(0xffffffffu, hi_i);
-        int wlo = 0, whi = 0;
-        if (hi_i >= 0) {
-            wlo = max(0, lo_i - (SINC ? 15 : 0));
-            whi = min(n, hi_i + (SINC ? 17 : 2));
-        }
-        const bool fits = whi - wlo <= F1_WMAX;
-        float2 *w = win[warp];
-        const float2 *row = a.sig + (size_t)i * n;
-        // the phase correction commutes with the (linear, per-pulse) interpolation: rotate the output
-        float2 rot = make_float2(1.f, 0.f);
-        if (a.theta) {
-            float sn, cs;
-            sincosf(a.theta[i], &sn, &cs);
-            rot = make_float2(cs, -sn);
-        }
-        if (fits)
-            for (int k = wlo + lane; k < whi; k += 32) w[k - wlo] = row[k];
-        __syncwarp();
+        prm[tid] = p;
+    }
+    // the query wavenumbers of this CTA's bins are the same for every pulse
+    double q[TB];
 #pragma unroll
-        for (int t = 0; t < F1_BINS / 32; ++t) {
-            const int jb = lane + 32 * t;
-            float2 out = make_float2(0.f, 0.f);
-            if (j0 + jb < n && jj[t] >= 0)
-                out = fits ? gather_f32<SINC>(w, wlo, n, jj[t], fr[t], tab) : gather_f32<SINC>(row, 0, n, jj[t], fr[t], tab);
-            tile[jb][slot] = a.theta ? cmul(out, rot) : out;
+    for (int t = 0; t < TB; ++t) {
+        const int j = j0 + lane + 32 * t;
+        q[t] = j < n ? a.kr_grid[j] : 0.0;
+    }
+    __syncthreads();
+
+    // start the copy of a window (every lane commits one group per slot, possibly empty)
+    auto fetch = [&](const F1Pulse &p, int wlo, int whi, float2 *w) {
+        if (p.i >= 0 && whi - wlo <= F1_WMAX) {
+            const float2 *row = a.sig + (size_t)p.i * n;
+            for (int k = wlo + lane; k < whi; k += 32) cp_async8(w + (k - wlo), row + k);
         }
-        __syncwarp();
+        cp_async_commit();
+    };
+
+    // iteration s brackets slot s and starts its window, then gathers slot s - 1 while that copy flies
+    int jj[TB], jn[TB];
+    Frac fr[TB], fn[TB];
+    int wlo = 0, whi = 0, wlo_n = 0, whi_n = 0;
+#pragma unroll
+    for (int s = 0; s <= SPW; ++s) {
+        if (s < SPW) {
+            // np.interp bracket of this warp's bins on pulse pn, and the sample window [wlo, whi) they read
+            const F1Pulse &pn = prm[warp + F1_WARPS * s];
+            wlo_n = whi_n = 0;
+            if (pn.i >= 0) {
+                auto kr = [&](int k) {
+                    return k == 0 ? pn.kfirst : (k == n - 1 ? pn.klast : pn.sc * (pn.f0 + (double)k * pn.df));
+                };
+                const bool asc = kr(n - 1) >= kr(0);
+                auto xa = [&](int t) { return asc ? kr(t) : kr(n - 1 - t); };
+                const double xa0 = xa(0), xa1 = xa(n - 1);
+                int lo_i = 1 << 30, hi_i = -1;
+#pragma unroll
+                for (int t = 0; t < TB; ++t) {
+                    jn[t] = -1;
+                    fn[t] = Frac{0.f, 0, 0};
+                    if (j0 + lane + 32 * t < n && q[t] >= xa0 && q[t] <= xa1) {
+                        // closed-form bracket on the affine axis; the end points are exact
+                        const double pos = (q[t] - xa0) * pn.inv_dk;
+                        const int ja = isfinite(pos) ? min(max((int)floor(pos), 0), n - 2) : 0;
+                        const double fd = (q[t] - xa(ja)) * pn.inv_dk;
+                        fn[t].f = (float)fd;
+                        fn[t].ph = sinc_phase(fd);
+                        // natural-order index of the lower sample and the weight toward the upper one
+                        int lowi;
+                        if (asc) { lowi = ja; } else { lowi = n - 2 - ja; mirror_frac(fn[t]); }
+                        jn[t] = lowi;
+                        lo_i = min(lo_i, lowi);
+                        hi_i = max(hi_i, lowi);
+                    }
+                }
+                lo_i = __reduce_min_sync(0xffffffffu, lo_i);
+                hi_i = __reduce_max_sync(0xffffffffu, hi_i);
+                if (hi_i >= 0) {
+                    wlo_n = max(0, lo_i - (SINC ? 15 : 0));
+                    whi_n = min(n, hi_i + (SINC ? 17 : 2));
+                }
+            } else {
+#pragma unroll
+                for (int t = 0; t < TB; ++t) jn[t] = -1;
+            }
+            fetch(pn, wlo_n, whi_n, win[warp][s & 1]);
+        }
+        if (s > 0) {
+            if (s < SPW) cp_async_wait_group<1>(); else cp_async_wait_group<0>();
+            __syncwarp();
+            const int slot = warp + F1_WARPS * (s - 1);
+            const F1Pulse &p = prm[slot];
+            if (p.i < 0) {
+#pragma unroll
+                for (int t = 0; t < TB; ++t) tile[lane + 32 * t][slot] = make_float2(0.f, 0.f);
+            } else {
+                const bool fits = whi - wlo <= F1_WMAX;
+                const float2 *w = win[warp][(s - 1) & 1];
+                const float2 *row = a.sig + (size_t)p.i * n;
+#pragma unroll
+                for (int t = 0; t < TB; ++t) {
+                    const int jb = lane + 32 * t;
+                    float2 out = make_float2(0.f, 0.f);
+                    if (jj[t] >= 0)
+                        out = fits ? gather_f32<SINC>(w, wlo, n, jj[t], fr[t], tab)
+                                   : gather_f32<SINC>(row, 0, n, jj[t], fr[t], tab);
+                    tile[jb][slot] = a.theta ? cmul(out, p.rot) : out;
+                }
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int t = 0; t < TB; ++t) {
+            jj[t] = jn[t];
+            fr[t] = fn[t];
+        }
+        wlo = wlo_n;
+        whi = whi_n;
     }
     __syncthreads();
     for (int jb = warp; jb < F1_BINS; jb += F1_WARPS) {
