@@ -99,30 +99,42 @@ __device__ __forceinline__ int interp_bracket(const F &xa, int n, double x0, dou
     return j;
 }
 
-// The same bracket for CH queries at once: every guess and both its end values are loaded before any is
-// tested, so the loads of the CH queries overlap; a query whose guess misses walks from it.
+// The same bracket for CH queries at once: the source values at guess - 1 .. guess + 2 are loaded for every
+// query before any is tested, so the loads of the CH queries overlap and a guess that is off by one (the
+// common miss of the affine guess on a tan(phi) axis) resolves without another round trip; a query that
+// misses by more walks from the guess.
 template <bool EXACT, int CH, class F>
 __device__ __forceinline__ void interp_brackets(const F &xa, int n, double x0, double x1, double inv_span,
                                                 const double (&x)[CH], const bool (&valid)[CH], int (&j)[CH],
                                                 Frac (&frac)[CH]) {
     int g[CH];
-    double a[CH], b[CH];
+    double v0[CH], v1[CH], v2[CH], v3[CH];
 #pragma unroll
     for (int c = 0; c < CH; ++c) {
         g[c] = (valid[c] && isfinite(inv_span)) ? min(max((int)((x[c] - x0) * inv_span), 0), n - 2) : 0;
-        a[c] = xa(g[c]);
-        b[c] = xa(g[c] + 1);
+        v0[c] = xa(max(g[c] - 1, 0));
+        v1[c] = xa(g[c]);
+        v2[c] = xa(g[c] + 1);
+        v3[c] = xa(min(g[c] + 2, n - 1));
     }
 #pragma unroll
     for (int c = 0; c < CH; ++c) {
         j[c] = -1;
         frac[c] = Frac{0.f, 0, 0};
         if (!valid[c] || !(x[c] >= x0) || !(x[c] <= x1)) continue;
-        if (a[c] <= x[c] && (x[c] < b[c] || g[c] == n - 2)) {
-            j[c] = g[c];
-            make_frac<EXACT>(x[c], a[c], b[c], frac[c]);
+        // j is the unique index in [0, n-2] with xa(j) <= x < xa(j+1) (x == xa(n-1) takes j = n-2)
+        const int gc = g[c];
+        if (v1[c] <= x[c] && (x[c] < v2[c] || gc == n - 2)) {
+            j[c] = gc;
+            make_frac<EXACT>(x[c], v1[c], v2[c], frac[c]);
+        } else if (gc + 1 <= n - 2 && v2[c] <= x[c] && (x[c] < v3[c] || gc + 1 == n - 2)) {
+            j[c] = gc + 1;
+            make_frac<EXACT>(x[c], v2[c], v3[c], frac[c]);
+        } else if (gc >= 1 && v0[c] <= x[c] && x[c] < v1[c]) {
+            j[c] = gc - 1;
+            make_frac<EXACT>(x[c], v0[c], v1[c], frac[c]);
         } else {
-            j[c] = interp_bracket<EXACT>(xa, n, x0, x1, x[c], g[c], frac[c]);
+            j[c] = interp_bracket<EXACT>(xa, n, x0, x1, x[c], gc, frac[c]);
         }
     }
 }

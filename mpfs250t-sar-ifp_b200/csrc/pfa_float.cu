@@ -270,7 +270,7 @@ k_fl_pass2_fft(FPass2Args a) {
     const double hn = a.window ? a.ham_n[j] : 1.0;
     int bl[E];      // packed bracket: lower natural index | phase << 16 | reversed << 24; -1 = outside
     float bf[E];    // lerp weight toward the upper sample
-    constexpr int CH = 4;
+    constexpr int CH = 2;
 #pragma unroll
     for (int u0 = 0; u0 < E; u0 += CH) {
         double q[CH];
@@ -519,7 +519,7 @@ __global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((
     const double lo_v = krj * a.tan_s[0], hi_v = krj * a.tan_s[m - 1];
     auto xa = [&](int t) { return krj * __ldg(a.tan_s + t); };
     const double inv_span = (double)(m - 1) / (hi_v - lo_v);
-    constexpr int CH = 4;
+    constexpr int CH = 2;
     for (int k0 = tid; k0 < m; k0 += CH * T) {
         double q[CH];
         bool ok[CH];
