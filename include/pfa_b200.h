@@ -80,9 +80,12 @@ typedef struct pfa_config {
     int32_t range_interp;  /* pfa_interp for pass 1 (--range-sinc)                          */
     int32_t az_interp;     /* pfa_interp for pass 2 (--az-sinc)                             */
     int32_t device;        /* CUDA device ordinal                                           */
-    int32_t fft_ept_cross; /* float: complex values per thread in the cross FFT (8 or 16; 0 = 16),
-                              i.e. CTA size pow2(m)/ept -- the tile shape the autotuner picks   */
-    int32_t fft_ept_range; /* float: same for the range FFT (pow2(n)/ept threads)               */
+    int32_t fft_ept_cross; /* float: complex values per thread in the cross FFT (8, 16 or 32;
+                              0 = automatic: 16; 8 applies to lines of 256..8192 points and 32 to
+                              lines of 8192 and 16384, other lines use 16), i.e. CTA size
+                              pow2(m)/ept -- the tile shape the autotuner picks                 */
+    int32_t fft_ept_range; /* float: same for the range FFT (pow2(n)/ept threads; 0 = automatic:
+                              32 for lines of 8192 and 16384 points, else 16)                    */
     int32_t detect_order;  /* fixed: pfa_detect_order (0 = emulator order)                      */
     int32_t reserved[6];
 } pfa_config;

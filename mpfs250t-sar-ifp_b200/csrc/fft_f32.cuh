@@ -10,7 +10,8 @@
 // so the result is in natural order and the last pass writes element (q, r) to index tid + T (q + r E/R):
 // callers store x[v] at frequency index tid + T v.  Pass 0 reads its operands straight from registers:
 // callers load x[u] with natural input index tid + T u.  Passes exchange through a padded shared buffer
-// of N + N/16 elements (index i stored at i + i/16: the pass-0 scatter with stride R is conflict free).
+// of N + N/16 elements (N + N/32 for E = 32; index i stored at i + i/16, resp. i + i/32: the pass-0
+// scatter with stride R is conflict free).
 // The twiddle table holds W_N^k = exp(-2 pi i k / N) for k < N.  The inverse transform is
 // conj(FFT(conj(x))) without scaling (callers conjugate on load and store).
 #pragma once
@@ -48,6 +49,32 @@ __device__ __forceinline__ float2 w16(int e) {
         case 14: return make_float2(h, h);
         default: return make_float2(c1, s1);
     }
+}
+
+// exp(-2 pi i e / 32) = cos(e pi / 16) - i sin(e pi / 16) for e = 0..31, from the cosines of the multiples
+// of pi/16 in [0, pi/2] (sin(k pi/16) = cos((8 - k) pi/16)) and the quadrant of e
+__device__ __forceinline__ float2 w32(int e) {
+    constexpr float c[9] = {1.f, 0.98078528040323044913f, 0.92387953251128675613f, 0.83146961230254523708f,
+                            0.70710678118654752440f, 0.55557023301960222474f, 0.38268343236508977173f,
+                            0.19509032201612826785f, 0.f};
+    e &= 31;
+    const int k = e & 7;
+    const float ck = c[k], sk = c[8 - k];
+    float cs, sn;                                   // cos and sin of e pi / 16
+    switch (e >> 3) {
+        case 0: cs = ck; sn = sk; break;
+        case 1: cs = -sk; sn = ck; break;
+        case 2: cs = -ck; sn = -sk; break;
+        default: cs = sk; sn = -ck; break;
+    }
+    return make_float2(cs, -sn);
+}
+
+// W_R^e for the radices used here (R divides 32)
+template <int R>
+__device__ __forceinline__ float2 wr(int e) {
+    if constexpr (R == 32) return w32(e);
+    else return w16(e * (16 / R));
 }
 
 // In-place DFT of size R on v (natural-order output), forward sign.
@@ -91,7 +118,7 @@ __device__ __forceinline__ void dft_split(float2 (&v)[R]) {
         for (int n2 = 0; n2 < Q; ++n2) t[n2] = v[n1 + P * n2];
         Dft<Q>::run(t);
 #pragma unroll
-        for (int k2 = 0; k2 < Q; ++k2) y[n1][k2] = (n1 * k2 == 0) ? t[k2] : cmul(t[k2], w16((n1 * k2) * (16 / R)));
+        for (int k2 = 0; k2 < Q; ++k2) y[n1][k2] = (n1 * k2 == 0) ? t[k2] : cmul(t[k2], wr<R>(n1 * k2));
     }
 #pragma unroll
     for (int k2 = 0; k2 < Q; ++k2) {
@@ -114,13 +141,20 @@ struct Dft<16> {
     __device__ static __forceinline__ void run(float2 (&v)[16]) { dft_split<16, 4, 4>(v); }
 };
 
+template <>
+struct Dft<32> {
+    __device__ static __forceinline__ void run(float2 (&v)[32]) { dft_split<32, 4, 8>(v); }
+};
+
 template <int L, int E>
 struct StockhamFft {
     static constexpr int N = 1 << L;
     static constexpr int T = N / E;
     static_assert(T >= 32, "at least one warp per line");
-    static constexpr int xbuf_elems() { return N + N / 16; }
-    __device__ static __forceinline__ int pad(int i) { return i + (i >> 4); }
+    // one pad element per PADW: the pass-0 scatter (stride R = E) stays free of bank conflicts
+    static constexpr int PADW = E >= 32 ? 32 : 16;
+    static constexpr int xbuf_elems() { return N + N / PADW; }
+    __device__ static __forceinline__ int pad(int i) { return i + i / PADW; }
 
     // radix of pass p: E while the remaining size allows, then the remainder
     static constexpr int radix(int p) {

@@ -177,14 +177,14 @@ pfa_status pfa_plan_create(const pfa_config *cfg, pfa_plan **out) {
         e = pfa::float_alloc(p->fl, c.m, c.n);
         p->fl.range_sinc = c.range_interp == PFA_INTERP_SINC;
         p->fl.az_sinc = c.az_interp == PFA_INTERP_SINC;
-        if ((c.fft_ept_cross != 0 && c.fft_ept_cross != 8 && c.fft_ept_cross != 16) ||
-            (c.fft_ept_range != 0 && c.fft_ept_range != 8 && c.fft_ept_range != 16)) {
+        auto ept_ok = [](int v) { return v == 0 || v == 8 || v == 16 || v == 32; };
+        if (!ept_ok(c.fft_ept_cross) || !ept_ok(c.fft_ept_range)) {
             pfa::float_free(p->fl);
             delete p;
             return PFA_ERR_BAD_CONFIG;
         }
-        p->fl.ept_cross = c.fft_ept_cross == 8 ? 8 : 16;
-        p->fl.ept_range = c.fft_ept_range == 8 ? 8 : 16;
+        p->fl.ept_cross = c.fft_ept_cross;      // 0: the automatic choice of the dispatch
+        p->fl.ept_range = c.fft_ept_range;
         p->ws_bytes = pfa::float_workspace_bytes(c.m, c.n);
         if (e == cudaErrorInvalidValue) { pfa::float_free(p->fl); delete p; return PFA_ERR_BAD_CONFIG; }
         if (e == cudaSuccess && c.mode == PFA_MODE_MIXED) {

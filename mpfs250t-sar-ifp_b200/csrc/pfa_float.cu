@@ -34,6 +34,12 @@ constexpr double kC = 299792458.0;
 template <int L, int E>
 using F32Fft = StockhamFft<L, E>;
 
+// resident CTAs per SM the line kernels are compiled for: 64 registers a thread for tiles of up to 16
+// values, 128 for the 32-value tile (its radix-32 passes hold 64 floats of data)
+constexpr int fl_min_ctas(int L, int E) {
+    return E >= 32 ? (((1 << L) / E >= 512) ? 1 : 2) : (((1 << L) / E >= 1024) ? 1 : (((1 << L) / E >= 512) ? 2 : 4));
+}
+
 // ------------------------------------------------------------------------------------------ K1f
 // Each warp owns a double-buffered window of its pulse's samples: the window of the next pulse streams
 // in (cp.async) while the current one is gathered.  The KR grid lies inside every pulse's own span, so
@@ -235,7 +241,7 @@ struct FPass2Args {
 constexpr int kCT = 8;
 
 template <int L, int E, bool SINC>
-__global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((1 << L) / E >= 512) ? 2 : 4))
+__global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, fl_min_ctas(L, E))
 k_fl_pass2_fft(FPass2Args a) {
     using F = F32Fft<L, E>;
     constexpr int N = F::N, T = F::T;
@@ -351,7 +357,7 @@ struct FFft2Args {
 };
 
 template <int L, int E>
-__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((1 << L) / E >= 512) ? 2 : 4)) k_fl_fft2(FFft2Args a) {
+__global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_fl_fft2(FFft2Args a) {
     using F = F32Fft<L, E>;
     constexpr int N = F::N, T = F::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -411,7 +417,7 @@ __device__ __forceinline__ void af_load_range_row(float2 (&x)[E], const AfRangeA
 }
 
 template <int L, int E>
-__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((1 << L) / E >= 512) ? 2 : 4)) k_af_entropy(AfRangeArgs a) {
+__global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_entropy(AfRangeArgs a) {
     using F = F32Fft<L, E>;
     constexpr int T = F::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -444,7 +450,7 @@ __global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((
 }
 
 template <int L, int E>
-__global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((1 << L) / E >= 512) ? 2 : 4))
+__global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, fl_min_ctas(L, E))
 k_af_range_adjoint(AfRangeArgs a) {
     namespace cg = cooperative_groups;
     using F = F32Fft<L, E>;
@@ -505,7 +511,7 @@ __device__ __forceinline__ int br_low(uint32_t p) { return (int)((p >> 17) & 0x3
 __device__ __forceinline__ float br_w(uint32_t p) { return (float)(p & 0x1ffffu) * (1.0f / 131071.f); }
 
 template <int L, int E>
-__global__ void __launch_bounds__((1 << L) / E, ((1 << L) / E >= 1024) ? 1 : (((1 << L) / E >= 512) ? 2 : 4)) k_af_cross_adjoint(AfCrossArgs a) {
+__global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_adjoint(AfCrossArgs a) {
     using F = F32Fft<L, E>;
     constexpr int N = F::N, T = F::T;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -628,12 +634,18 @@ cudaError_t launch_fft2(const FloatDev &d, void *out, int detect, float scale, c
     return cudaGetLastError();
 }
 
-// FFT register tile: 16 complex values per thread by default, 8 on request (twice the CTA size) for
-// lines of 256 points and more
+// FFT register tile: 16 complex values per thread; 8 on request (twice the CTA size) for lines of 256
+// points and more; 32 (half the CTA size, radix-32 passes: one shared-memory exchange fewer) for lines
+// of 8192 and 16384 points, on request and by default for the range FFT (0 = automatic).  The cross
+// FFT of pass 2 stays at 16 by default: that kernel is latency bound and loses more to the halved
+// CTA than it gains from the saved exchange.
 template <int L, bool SINC>
 cudaError_t pass2_tile(const FloatDev &d, cudaStream_t st) {
     if constexpr (L >= 8 && L <= 13) {      // 2^L / 8 threads must stay within a CTA's 1024
         if (d.ept_cross == 8) return launch_pass2<L, 8, SINC>(d, st);
+    }
+    if constexpr (L >= 13) {
+        if (d.ept_cross == 32) return launch_pass2<L, 32, SINC>(d, st);
     }
     return launch_pass2<L, Cfg<L>::E, SINC>(d, st);
 }
@@ -642,6 +654,9 @@ template <int L>
 cudaError_t fft2_tile(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st) {
     if constexpr (L >= 8 && L <= 13) {
         if (d.ept_range == 8) return launch_fft2<L, 8>(d, out, detect, scale, st);
+    }
+    if constexpr (L >= 13) {               // the automatic choice (0) for these lines: 32 (measured faster)
+        if (d.ept_range == 32 || d.ept_range == 0) return launch_fft2<L, 32>(d, out, detect, scale, st);
     }
     return launch_fft2<L, Cfg<L>::E>(d, out, detect, scale, st);
 }

@@ -46,7 +46,7 @@ struct FloatDev {
     float2 *p1 = nullptr;              // [n][mpad] pass-1 output (range-bin rows, sorted pulses)
     float2 *y1 = nullptr;              // [m2][npad] cross FFT output, transposed (cross-bin rows)
     int kr_positive = 0;               // KR > 0 everywhere (ascending pass-2 sources)
-    int ept_cross = 16, ept_range = 16;  // FFT register tile (complex values per thread)
+    int ept_cross = 0, ept_range = 0;    // FFT register tile (complex values per thread; 0 = automatic)
     float2 *af_zadj = nullptr;         // [n][m2] autofocus: adjoint of the range FFT (range-bin rows)
     double *af_acc = nullptr;          // [2] sum I, sum I log I
     float *af_dacc = nullptr;          // [mpad] per-slot gradient accumulators

@@ -1,7 +1,7 @@
 """Project autotuner for the float engine.
 
 The tunable tile of the float path is the FFT register tile: complex values per thread of the cross
-FFT (fused with pass 2) and of the range FFT, 8 or 16, which sets the CTA size (line length / tile)
+FFT (fused with pass 2) and of the range FFT, 8, 16 or 32, which sets the CTA size (line length / tile)
 and so the register/occupancy/barrier trade-off.  ``tune_float`` times every candidate on the device
 for one scene shape (CUDA events, median of ``reps`` frames after a warm-up) and returns the fastest.
 Results are cached per (pow2 m, pow2 n, interpolators) in memory and in a JSON file
@@ -17,7 +17,7 @@ from pathlib import Path
 from .engine import FloatPlan
 from .geometry import pow2
 
-CANDIDATES = ((16, 16), (8, 16), (16, 8), (8, 8))
+CANDIDATES = ((16, 16), (8, 16), (16, 8), (8, 8), (16, 32))
 _MEM: dict = {}
 
 

@@ -27,7 +27,7 @@ class BatchFormer:
         self.plans = []
         for i, (tb, sig) in enumerate(scenes):
             m, n = tuple(sig.shape)
-            tile = tiles[i] if tiles is not None else (16, 16)
+            tile = tiles[i] if tiles is not None else (0, 0)
             p = FloatPlan(m, n, range_sinc, az_sinc, mixed=mixed, device=device, tile=tile)
             p.set_tables(tb)
             self.plans.append(p)

@@ -191,8 +191,9 @@ class FloatPlan(_Plan):
     DETECT = {"mag": _lib.DETECT_MAG, "power": _lib.DETECT_POWER, "complex": _lib.DETECT_COMPLEX}
 
     def __init__(self, m: int, n: int, range_sinc: bool = False, az_sinc: bool = False, mixed: bool = False,
-                 device: int = 0, tile: tuple = (16, 16)):
-        """``tile``: complex values per thread of the (cross, range) FFTs, 8 or 16 (the autotuner's knob)."""
+                 device: int = 0, tile: tuple = (0, 0)):
+        """``tile``: complex values per thread of the (cross, range) FFTs, 8, 16 or 32, 0 = the library's
+        automatic choice (the autotuner's knob)."""
         cfg = _lib.Config(mode=_lib.MODE_MIXED if mixed else _lib.MODE_FLOAT32, m=m, n=n, grid=0,
                           range_interp=_lib.SINC if range_sinc else _lib.LERP,
                           az_interp=_lib.SINC if az_sinc else _lib.LERP, device=device,

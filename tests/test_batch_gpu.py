@@ -28,6 +28,19 @@ def test_tile_variants_match_fp64(torch_cuda, tile):
     assert fp.rel_l2(cz, r64) <= 1e-6
 
 
+# the 32-value tile (radix-32 passes) exists for lines of 8192 and 16384 points: cross lines of 8192
+# (4500 pulses), range lines of 8192 (4500 samples) and cross lines of 16384 (8200 pulses)
+@pytest.mark.parametrize("m,n,tile", [(4500, 600, (32, 16)), (700, 4500, (16, 32)), (8200, 500, (32, 32))])
+def test_tile32_matches_fp64(torch_cuda, m, n, tile):
+    sc = synth.make_scene(m, n, n_targets=16, clutter_db=-10.0, snr_db=20.0, seed=63, jitter=0.3)
+    tb = geometry.prepare_tables_from_scene(sc)
+    with engine.FloatPlan(m, n, tile=tile) as plan:
+        plan.set_tables(tb)
+        cz = plan.form(sc.signal, detect="complex")
+    r64 = fp.pfa_image(sc.signal, tb["freq"], tb["ax"], tb["ay"], tb["sgn"], precision="f64")
+    assert fp.rel_l2(cz, r64) <= 1e-6
+
+
 def test_autotuner_picks_a_candidate(torch_cuda, tmp_path, monkeypatch):
     torch = torch_cuda
     monkeypatch.setenv("PFA_TUNE_CACHE", str(tmp_path / "tune.json"))
