@@ -246,6 +246,13 @@ struct Pass1Args {
     int cubic;                        // 4-tap Lagrange instead of the lerp (SINC off)
 };
 
+// per-slot pulse constants, computed once per CTA
+struct P1Pulse {
+    double fac, f0, df, inv_step, c0;
+    int i;                            // source pulse, -1 for a slot past the last pulse
+    int asc;
+};
+
 constexpr size_t P1_SMEM_TILE = (size_t)P1_BINS * (P1_SLOTS + 1) * 4;
 constexpr size_t P1_SMEM_WIN = (size_t)P1_WARPS * P1_WMAX * 8;   // int32 I/Q pairs
 constexpr size_t p1_smem(bool sinc) { return P1_SMEM_TILE + P1_SMEM_WIN + (sinc ? 2 * 256 * kSincTaps : 0); }
@@ -265,24 +272,48 @@ __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
         uint32_t *dst = reinterpret_cast<uint32_t *>(tab);
         for (int i = tid; i < 256 * kSincTaps / 2; i += blockDim.x) dst[i] = src[i];
     }
+    __shared__ P1Pulse prm[P1_SLOTS];
+    if (tid < P1_SLOTS) {
+        P1Pulse p{};
+        p.i = -1;
+        const int r = r0 + tid;
+        if (r < a.m) {
+            const int i = a.order[r];
+            p.i = i;
+            p.fac = (double)a.fac[i];
+            p.f0 = (double)a.f0[i];
+            p.df = (double)a.df[i];
+            // kr_i[k] = f64(fac) * (f64(f0) + f64(k) * f64(df))   (silicon_emulator.py:144)
+            auto kr = [&](int k) { return __dmul_rn(p.fac, __dadd_rn(p.f0, __dmul_rn((double)k, p.df))); };
+            p.asc = kr(n - 1) >= kr(0);
+            p.inv_step = 1.0 / (p.fac * p.df);      // affine-estimate coefficients (guess only)
+            p.c0 = p.f0 / p.df;
+        }
+        prm[tid] = p;
+    }
+    // the query wavenumbers of this CTA's bins are the same for every pulse
+    double qv[P1_BINS / 32];
+#pragma unroll
+    for (int t = 0; t < P1_BINS / 32; ++t) {
+        const int j = j0 + lane + 32 * t;
+        qv[t] = j < n ? (double)a.krp[j] : 0.0;
+    }
     const float lsb = a.sig ? (float)ldexp(1.0, a.ctrl[3]) : 1.0f;
     __syncthreads();
 
     for (int s = 0; s < P1_SLOTS / P1_WARPS; ++s) {
         const int slot = warp + P1_WARPS * s;
-        const int r = r0 + slot;
-        if (r >= a.m) {
+        const P1Pulse &p = prm[slot];
+        if (p.i < 0) {
             for (int t = lane; t < P1_BINS; t += 32) tile[t][slot] = 0u;
             continue;
         }
-        const int i = a.order[r];
-        const double fac = (double)a.fac[i], f0 = (double)a.f0[i], df = (double)a.df[i];
-        // kr_i[k] = f64(fac) * (f64(f0) + f64(k) * f64(df))   (silicon_emulator.py:144)
+        const int i = p.i;
+        const double fac = p.fac, f0 = p.f0, df = p.df;
         auto kr = [&](int k) { return __dmul_rn(fac, __dadd_rn(f0, __dmul_rn((double)k, df))); };
-        const bool asc = kr(n - 1) >= kr(0);
+        const bool asc = p.asc;
         auto xa = [&](int t) { return asc ? kr(t) : kr(n - 1 - t); };
-        const double inv_step = 1.0 / (fac * df);     // affine-estimate coefficients (guess only)
-        const double c0 = f0 / df;
+        const double inv_step = p.inv_step, c0 = p.c0;
         Bracket br[P1_BINS / 32];
         int lo_i = 1 << 30, hi_i = -1;
 #pragma unroll
@@ -290,7 +321,7 @@ __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
             const int j = j0 + lane + 32 * t;
             br[t] = Bracket{-1, 0};
             if (j < n) {
-                const double q = (double)a.krp[j];
+                const double q = qv[t];
                 const double kest = q * inv_step - c0;     // affine estimate of the source index
                 int g = 0;
                 if (isfinite(kest) && isfinite(inv_step)) {
