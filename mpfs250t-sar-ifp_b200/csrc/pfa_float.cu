@@ -561,8 +561,11 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
     }
     __syncthreads();
     // R2^H, atomics free: slot r collects bracket k with lower index r (weight 1-f) and r-1 (weight f);
-    // the lower index is monotone in k, so each thread walks one contiguous run of k for its 16 slots
+    // the lower index is monotone in k, so each thread walks one contiguous run of k for its E slots
     const int r_lo = tid * E;
+    float2 gs[E];
+#pragma unroll
+    for (int s2 = 0; s2 < E; ++s2) gs[s2] = make_float2(0.f, 0.f);
     if (r_lo < m) {
         int lo = 0, hi = m;                             // first k with lower index >= r_lo - 1
         while (lo < hi) {
@@ -570,26 +573,46 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
             if (br_low(pk[mid]) < r_lo - 1) lo = mid + 1; else hi = mid;
         }
         int kp = lo;
-        const float2 *p1row = a.p1 + (size_t)j * a.mpad;
-#pragma unroll 1
+#pragma unroll
         for (int s2 = 0; s2 < E; ++s2) {
             const int r = r_lo + s2;
-            if (r >= m) break;
-            float2 gsum = make_float2(0.f, 0.f);
-            for (int kk = kp; kk < m; ++kk) {
-                const uint32_t b = pk[kk];
-                const int l = br_low(b);
-                if (l > r) break;
-                if (b >> 31) continue;
-                const float f = br_w(b);
-                const float wgt = (l == r) ? 1.0f - f : (l == r - 1 ? f : 0.f);
-                const float2 y = xbuf[kk];
-                gsum.x = fmaf(wgt, y.x, gsum.x);
-                gsum.y = fmaf(wgt, y.y, gsum.y);
+            if (r < m) {
+                float2 gsum = make_float2(0.f, 0.f);
+                for (int kk = kp; kk < m; ++kk) {
+                    const uint32_t b = pk[kk];
+                    const int l = br_low(b);
+                    if (l > r) break;
+                    if (b >> 31) continue;
+                    const float f = br_w(b);
+                    const float wgt = (l == r) ? 1.0f - f : (l == r - 1 ? f : 0.f);
+                    const float2 y = xbuf[kk];
+                    gsum.x = fmaf(wgt, y.x, gsum.x);
+                    gsum.y = fmaf(wgt, y.y, gsum.y);
+                }
+                while (kp < m && br_low(pk[kp]) < r) ++kp;
+                gs[s2] = gsum;
             }
-            while (kp < m && br_low(pk[kp]) < r) ++kp;
-            const float2 pv = p1row[r];
-            atomicAdd(a.dacc + r, gsum.x * pv.y - gsum.y * pv.x);   // Im(conj(g) p1)
+        }
+    }
+    // the slot sums go through shared memory (padded: a thread's E consecutive slots hit distinct banks)
+    // so that the p1 loads and the accumulation run slot-coalesced, all of a thread's loads in flight
+    __syncthreads();
+#pragma unroll
+    for (int s2 = 0; s2 < E; ++s2) xbuf[F::pad(r_lo + s2)] = gs[s2];
+    __syncthreads();
+    const float2 *p1row = a.p1 + (size_t)j * a.mpad;
+    float2 pv[E];
+#pragma unroll
+    for (int v = 0; v < E; ++v) {
+        const int r = tid + T * v;
+        pv[v] = r < m ? __ldcs(p1row + r) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int v = 0; v < E; ++v) {
+        const int r = tid + T * v;
+        if (r < m) {
+            const float2 g = xbuf[F::pad(r)];
+            atomicAdd(a.dacc + r, g.x * pv[v].y - g.y * pv[v].x);   // Im(conj(g) p1)
         }
     }
 }
