@@ -368,7 +368,7 @@ def run_ours(a, ws, rank, local):
     outs_host = [torch.empty(tuple(img.shape), dtype=img.dtype).pin_memory() for _ in range(2)]
     sig_np = sig_host.numpy()
     outs_np = [o.numpy() for o in outs_host]
-    ne2e = max(4, min(a.steps, 8))
+    ne2e = max(4, min(a.steps, 16))
     frames_in = [sig_np] * ne2e
     frames_out = [outs_np[k & 1] for k in range(ne2e)]
     for _ in range(2):

@@ -152,6 +152,11 @@ __global__ void __launch_bounds__(256, SINC ? 3 : 4) k_fl_pass1(FPass1Args a) {
                 const bool asc = kr(n - 1) >= kr(0);
                 auto xa = [&](int t) { return asc ? kr(t) : kr(n - 1 - t); };
                 const double xa0 = xa(0), xa1 = xa(n - 1);
+                const bool fin = isfinite(pn.inv_dk);
+                // xa(ja) for ja in [0, n-2]: xa0 at ja = 0 (the exact end point), the affine model inside
+                auto xa_lo = [&](int ja) {
+                    return ja == 0 ? xa0 : pn.sc * (pn.f0 + (double)(asc ? ja : n - 1 - ja) * pn.df);
+                };
                 int lo_i = 1 << 30, hi_i = -1;
 #pragma unroll
                 for (int t = 0; t < TB; ++t) {
@@ -160,8 +165,8 @@ __global__ void __launch_bounds__(256, SINC ? 3 : 4) k_fl_pass1(FPass1Args a) {
                     if (j0 + lane + 32 * t < n && q[t] >= xa0 && q[t] <= xa1) {
                         // closed-form bracket on the affine axis; the end points are exact
                         const double pos = (q[t] - xa0) * pn.inv_dk;
-                        const int ja = isfinite(pos) ? min(max((int)floor(pos), 0), n - 2) : 0;
-                        const double fd = (q[t] - xa(ja)) * pn.inv_dk;
+                        const int ja = fin ? min(max((int)floor(pos), 0), n - 2) : 0;
+                        const double fd = (q[t] - xa_lo(ja)) * pn.inv_dk;
                         fn[t].f = (float)fd;
                         fn[t].ph = sinc_phase(fd);
                         // natural-order index of the lower sample and the weight toward the upper one
@@ -217,11 +222,13 @@ __global__ void __launch_bounds__(256, SINC ? 3 : 4) k_fl_pass1(FPass1Args a) {
         whi = whi_n;
     }
     __syncthreads();
-    for (int jb = warp; jb < F1_BINS; jb += F1_WARPS) {
+    // two slots per lane, two bins per warp store (mpad is a multiple of 32: every slot of the CTA exists)
+    const int half = lane >> 4, l2 = 2 * (lane & 15);
+    for (int jb = 2 * warp + half; jb < F1_BINS; jb += 2 * F1_WARPS) {
         const int j = j0 + jb;
         if (j >= n) break;
-        const int r = r0 + lane;
-        if (r < a.mpad) a.p1[(size_t)j * a.mpad + r] = tile[jb][lane];
+        const float2 u0 = tile[jb][l2], u1 = tile[jb][l2 + 1];
+        *reinterpret_cast<float4 *>(a.p1 + (size_t)j * a.mpad + r0 + l2) = make_float4(u0.x, u0.y, u1.x, u1.y);
     }
 }
 
