@@ -392,12 +392,14 @@ __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
         __syncwarp();
     }
     __syncthreads();
-    // corner turn #1: range-bin rows, sorted-slot columns, 128 B per row segment
-    for (int jj = warp; jj < P1_BINS; jj += P1_WARPS) {
+    // corner turn #1: range-bin rows, sorted-slot columns, 128 B per row segment; four slots per lane,
+    // four bins per warp store (mpad is a multiple of 32: every slot of the CTA exists)
+    const int quarter = lane >> 3, l4 = 4 * (lane & 7);
+    for (int jj = 4 * warp + quarter; jj < P1_BINS; jj += 4 * P1_WARPS) {
         const int j = j0 + jj;
         if (j >= n) break;
-        const int r = r0 + lane;
-        if (r < a.mpad) a.p1[(size_t)j * a.mpad + r] = tile[jj][lane];
+        *reinterpret_cast<uint4 *>(a.p1 + (size_t)j * a.mpad + r0 + l4) =
+            make_uint4(tile[jj][l4], tile[jj][l4 + 1], tile[jj][l4 + 2], tile[jj][l4 + 3]);
     }
 }
 
