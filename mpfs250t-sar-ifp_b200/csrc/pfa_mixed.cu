@@ -2,7 +2,7 @@
 // transform2d :144-147) as fp16 hi/lo DFT-matrix products on the tcgen05 tensor cores with fp32
 // accumulation (fft_tc.cuh); resampling, window and detection stay FP32 with FP64 coordinates.
 //
-//   k_mx_pass2<L,SINC>  persistent 8-CTA clusters: per range bin the pass-2 gather (as k_fl_pass2_fft),
+//   k_mx_pass2<L,SINC>  persistent 4-CTA clusters: per range bin the pass-2 gather (as k_fl_pass2_fft),
 //                       the cross FFT on the tensor cores, and corner turn #2 through distributed shared
 //                       memory into the transposed buffer y1t [cross bin][npad]
 //   k_mx_fft2<L>        persistent CTAs: per cross bin the range FFT on the tensor cores and the
@@ -32,7 +32,7 @@ namespace {
 using tcfft::Geo;
 using tcfft::TcFft;
 
-constexpr int kMxCT = 8;                      // cluster size of the mixed pass 2
+constexpr int kMxCT = 4;                      // cluster size of the mixed pass 2 (divides 8: npad holds whole clusters)
 constexpr size_t kMxMinSmem = 118 * 1024;     // > half of the SM's shared memory: one CTA per SM
 
 __host__ __device__ constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
@@ -357,7 +357,7 @@ __global__ void __cluster_dims__(kMxCT, 1, 1) __launch_bounds__(Geo<L>::THREADS,
         for (int s2 = 0; s2 < N / T; ++s2) {
             const int item = tid + T * s2;
             const int r8 = item & (kMxCT - 1);
-            const int k = rank * (N / kMxCT) + (item >> 3);
+            const int k = rank * (N / kMxCT) + item / kMxCT;
             const float2 *remote = cluster.map_shared_rank(reinterpret_cast<float2 *>(b2), r8);
             const int pos = 2 * tcfft::swz_chunk<ilog2c(N2 / 2)>(k >> 1) + (k & 1);
             a.y1t[(size_t)k * a.npad + grp * kMxCT + r8] = remote[pos];
