@@ -172,6 +172,19 @@ def _device_ms(fn, steps, warmup):
     return e0.elapsed_time(e1) / steps
 
 
+def cpu_float_small(sc, tables):
+    """CPU baseline of the small float scene: the oracle's restatement of form_image_pfa (np.interp
+    passes, float32 window, NumPy 2 single-precision FFT, |z|), lerp, whole frame, one core, best of 3."""
+    from oracle import float_pfa as fp
+    best = float("inf")
+    for _ in range(3):
+        t0 = time.perf_counter()
+        fp.detect(fp.pfa_image(sc.signal, tables["freq"], tables["ax"], tables["ay"], tables["sgn"], precision="ref"))
+        best = min(best, time.perf_counter() - t0)
+    return {"value": round(best * 1000.0, 1), "unit": "ms/frame", "cores": 1, "kind": "port",
+            "sample": "whole 1024x1024 frame, form_image_pfa restated (lerp), best of 3"}
+
+
 def measure_modes(a, local):
     """The other configurations of the metric, device-timed at N=1: the NDSU-shaped float frame
     (8167x8192 -> 8192^2; FP32 lerp as form_image_pfa, FP32 32-tap sinc, and both in the split-precision
@@ -180,9 +193,23 @@ def measure_modes(a, local):
     import numpy as np
     import torch
     from pfa_b200 import autofocus, engine, geometry, synth
-    from oracle import autofocus_ref
     steps = max(3, min(a.steps, 10))
     out = {}
+    # the small float scene (1024x1024, 64 targets, 20 dB SNR): lerp as form_image_pfa and the float sinc,
+    # inputs (8 MB) L2 resident, with the CPU restatement of form_image_pfa timed beside it
+    sc1 = synth.workload_scene("small_1024")
+    tb1 = geometry.prepare_tables_from_scene(sc1)
+    sig1 = torch.from_numpy(np.ascontiguousarray(sc1.signal, np.complex64)).to(f"cuda:{local}")
+    small = {"workload": "small_1024: 1024x1024 c64 -> 1024^2, 64 targets, 20 dB SNR (inputs L2 resident)"}
+    for nm, rs in (("lerp", False), ("sinc", True)):
+        with engine.FloatPlan(1024, 1024, rs, rs, device=local) as plan:
+            plan.set_tables(tb1)
+            img = torch.empty((1024, 1024), dtype=torch.float32, device=sig1.device)
+            small[f"ms_per_frame_{nm}"] = round(_device_ms(lambda: plan.form(sig1, out=img), 20, 5), 4)
+    if not a.no_cpu_baseline:
+        small["cpu_baseline"] = cpu_float_small(sc1, tb1)
+    out["small_1024"] = small
+    del sig1
     sc, sig = synth.make_scene_device(8167, 8192, device=f"cuda:{local}", **{k: v for k, v in synth.WORKLOADS["ndsu_8167x8192"].items() if k not in ("m", "n")})
     tables = geometry.prepare_tables_from_scene(sc)
     ref_c = {}
@@ -228,7 +255,7 @@ def measure_modes(a, local):
     del sig
     wl = synth.WORKLOADS["autofocus_4096"]
     sc, sig = synth.make_scene_device(4096, 4096, device=f"cuda:{local}", **{k: v for k, v in wl.items() if k not in ("m", "n")})
-    phi = torch.as_tensor(autofocus_ref.phase_error(4096, seed=4), device=sig.device)
+    phi = torch.as_tensor(synth.phase_error(4096, seed=4), device=sig.device)
     sig = (sig * torch.polar(torch.ones_like(phi), phi)[:, None].to(torch.complex64)).contiguous()
     tables = geometry.prepare_tables_from_scene(sc)
     with engine.FloatPlan(4096, 4096, device=local) as plan:

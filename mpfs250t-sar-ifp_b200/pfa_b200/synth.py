@@ -232,3 +232,11 @@ class FakeReader:
 
     def close(self):
         pass
+
+
+def phase_error(m: int, seed: int = 4, quad_edge: float = 3.0, walk_std: float = 0.05) -> np.ndarray:
+    """The autofocus workload's injected per-pulse phase error (float64, radians): quadratic with
+    `quad_edge` rad at the aperture edges plus a random walk of `walk_std` rad/pulse (seeded)."""
+    rng = np.random.default_rng(seed)
+    u = np.linspace(-1.0, 1.0, m)
+    return quad_edge * u * u + np.cumsum(rng.normal(0.0, walk_std, m))

@@ -157,3 +157,10 @@ def test_variant_frames_are_consistent():
     fused, _ = fe.form_image(sc.signal, tb, 128, True, True, detect_order="fused")
     d = np.abs(emu.astype(np.int64) - fused.astype(np.int64))
     assert d.max() <= 2 and (d > 0).any()
+
+
+def test_synth_phase_error_matches_autofocus_oracle():
+    """The bench's injected autofocus phase error (pfa_b200.synth) is the oracle's (autofocus_ref)."""
+    from oracle import autofocus_ref
+    for m, seed in ((4096, 4), (256, 7)):
+        assert np.array_equal(synth.phase_error(m, seed=seed), autofocus_ref.phase_error(m, seed=seed))
