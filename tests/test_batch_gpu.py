@@ -41,6 +41,24 @@ def test_tile32_matches_fp64(torch_cuda, m, n, tile):
     assert fp.rel_l2(cz, r64) <= 1e-6
 
 
+def test_tile_values_checked(torch_cuda):
+    """Tiles other than 0 (automatic), 8, 16 and 32 are a configuration error; 32 on lines it does not
+    apply to (here 1024 points) runs the 16-value tile."""
+    from pfa_b200 import _lib
+    for bad in ((24, 16), (16, 4), (64, 64)):
+        with pytest.raises(_lib.PfaError) as ei:
+            engine.FloatPlan(600, 900, tile=bad)
+        assert ei.value.status == _lib.BAD_CONFIG
+    sc = synth.make_scene(600, 900, n_targets=8, seed=64)
+    tb = geometry.prepare_tables_from_scene(sc)
+    out = []
+    for tile in ((32, 32), (16, 16)):
+        with engine.FloatPlan(600, 900, tile=tile) as plan:
+            plan.set_tables(tb)
+            out.append(plan.form(sc.signal, detect="complex").cpu().numpy())
+    assert np.array_equal(out[0], out[1])
+
+
 def test_autotuner_picks_a_candidate(torch_cuda, tmp_path, monkeypatch):
     torch = torch_cuda
     monkeypatch.setenv("PFA_TUNE_CACHE", str(tmp_path / "tune.json"))
