@@ -518,6 +518,12 @@ __device__ __forceinline__ uint32_t pack_br(int dead, int lowi, float f) {
     return ((uint32_t)dead << 31) | ((uint32_t)lowi << 17) | q;
 }
 __device__ __forceinline__ int br_low(uint32_t p) { return (int)((p >> 17) & 0x3fffu); }
+// Shared-memory positions of bracket k and of W . F^H g at cross index k in the cross adjoint.  Its
+// segmented reduction has lane t walk indices near 16 t; XOR-ing the low four index bits with bits of
+// the group index (a permutation inside each aligned group of 16) spreads those lanes over the banks
+// (4-byte brackets: bits 5..8; 8-byte values: bits 4..7), and consecutive writers stay conflict free.
+__device__ __forceinline__ int pk_at(int k) { return k ^ ((k >> 5) & 15); }
+__device__ __forceinline__ int y_at(int k) { return k ^ ((k >> 4) & 15); }
 __device__ __forceinline__ float br_w(uint32_t p) { return (float)(p & 0x1ffffu) * (1.0f / 131071.f); }
 
 template <int L, int E>
@@ -549,7 +555,7 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
         interp_brackets<false, CH>(xa, m, lo_v, hi_v, inv_span, q, ok, ja, fr);
 #pragma unroll
         for (int c = 0; c < CH; ++c)
-            if (ok[c]) pk[k0 + c * T] = ja[c] >= 0 ? pack_br(0, ja[c], fr[c].f) : pack_br(1, q[c] < lo_v ? 0 : m - 2, 0.f);
+            if (ok[c]) pk[pk_at(k0 + c * T)] = ja[c] >= 0 ? pack_br(0, ja[c], fr[c].f) : pack_br(1, q[c] < lo_v ? 0 : m - 2, 0.f);
     }
     // adjoint of the cross FFT
     const float2 *row = a.zadj_t + (size_t)j * N;
@@ -567,7 +573,7 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
         const int k = tid + T * v;
         float w = 0.f;
         if (k < m) w = a.window ? (float)(a.ham_m[k] * hn) : 1.0f;
-        xbuf[k] = make_float2(w * x[v].x, -w * x[v].y);      // W . F_cross^H g, cross index k
+        xbuf[y_at(k)] = make_float2(w * x[v].x, -w * x[v].y);   // W . F_cross^H g, cross index k
     }
     __syncthreads();
     // R2^H, atomics free: slot r collects bracket k with lower index r (weight 1-f) and r-1 (weight f);
@@ -580,7 +586,7 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
         int lo = 0, hi = m;                             // first k with lower index >= r_lo - 1
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
-            if (br_low(pk[mid]) < r_lo - 1) lo = mid + 1; else hi = mid;
+            if (br_low(pk[pk_at(mid)]) < r_lo - 1) lo = mid + 1; else hi = mid;
         }
         int kp = lo;
 #pragma unroll
@@ -589,17 +595,17 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
             if (r < m) {
                 float2 gsum = make_float2(0.f, 0.f);
                 for (int kk = kp; kk < m; ++kk) {
-                    const uint32_t b = pk[kk];
+                    const uint32_t b = pk[pk_at(kk)];
                     const int l = br_low(b);
                     if (l > r) break;
                     if (b >> 31) continue;
                     const float f = br_w(b);
                     const float wgt = (l == r) ? 1.0f - f : (l == r - 1 ? f : 0.f);
-                    const float2 y = xbuf[kk];
+                    const float2 y = xbuf[y_at(kk)];
                     gsum.x = fmaf(wgt, y.x, gsum.x);
                     gsum.y = fmaf(wgt, y.y, gsum.y);
                 }
-                while (kp < m && br_low(pk[kp]) < r) ++kp;
+                while (kp < m && br_low(pk[pk_at(kp)]) < r) ++kp;
                 gs[s2] = gsum;
             }
         }
@@ -825,7 +831,7 @@ template <int L>
 cudaError_t launch_af_cross(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, Cfg<L>::E>;
     AfCrossArgs p{d.af_zadj, d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.twm, d.af_dacc, d.m, d.n, d.mpad, d.window};
-    const size_t sm = (size_t)8 * F::xbuf_elems() + (size_t)4 * d.m;
+    const size_t sm = (size_t)8 * F::xbuf_elems() + (size_t)4 * ((d.m + 15) & ~15);   // pk: whole groups of 16
     auto fn = k_af_cross_adjoint<L, Cfg<L>::E>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;

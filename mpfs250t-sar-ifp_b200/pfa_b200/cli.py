@@ -6,8 +6,9 @@
 
 The input is a seeded synthetic scene of the given shape (or ``--input`` a complex64 .npy phase history
 with ``--tables`` an .npz of ``prepare_tables`` output).  Prints the device time of every frame; ``--out``
-saves the last image.  Modes: ``fixed`` (bit-exact emulator datapath), ``float`` (FP32) and ``mixed``
-(split-precision tensor-core FFTs).
+saves the last image.  Modes: ``fixed`` (bit-exact emulator datapath), ``float`` (FP32), ``mixed``
+(split-precision tensor-core FFTs) and ``autofocus`` (the image-entropy gradient w.r.t. the per-pulse
+phase of a scene with the injected quadratic + random-walk phase error; one gradient per frame).
 """
 from __future__ import annotations
 
@@ -19,7 +20,7 @@ import numpy as np
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--mode", choices=("fixed", "float", "mixed"), default="float")
+    ap.add_argument("--mode", choices=("fixed", "float", "mixed", "autofocus"), default="float")
     ap.add_argument("--m", type=int, default=2048, help="pulses")
     ap.add_argument("--n", type=int, default=2048, help="samples per pulse")
     ap.add_argument("--grid", type=int, default=0, help="fixed mode: square output raster (default pow2)")
@@ -49,6 +50,21 @@ def main(argv=None) -> int:
                                           snr_db=15.0, seed=a.seed)
         tb = geometry.prepare_tables_from_scene(sc)
     m, n = sig.shape
+    if a.mode == "autofocus":
+        from . import autofocus
+        phi = torch.as_tensor(synth.phase_error(m, seed=a.seed), device=dev)
+        sig = (sig * torch.polar(torch.ones_like(phi), phi)[:, None].to(torch.complex64)).contiguous()
+        theta = torch.zeros(m, dtype=torch.float32, device=dev)
+        with engine.FloatPlan(m, n, device=a.device) as plan:
+            plan.set_tables(tb)
+            for k in range(a.frames):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                ent, dth = autofocus.entropy_grad(plan, sig, theta)
+                e1.record()
+                torch.cuda.synchronize()
+                print(f"gradient {k}: {e0.elapsed_time(e1):.3f} ms  (entropy {float(ent):.5f}, {m}x{n})")
+        return 0
     if a.mode == "fixed":
         grid = a.grid or geometry.pow2(max(m, n))
         plan = engine.FixedPlan(m, n, grid, a.range_sinc, a.az_sinc, device=a.device)
