@@ -155,6 +155,44 @@ __device__ __forceinline__ uint32_t sinc_gather(const W *win, int base, int sn, 
     return pack16(sat16(ar + (((br - ar) * b.wq) >> 15)), sat16(ai + (((bi - ai) * b.wq) >> 15)));
 }
 
+// The same gather with the table in shared memory as phase-major rows of kSincRow int16 (taps 0..31,
+// then padding): a lane reads its phase's 32 taps as four 16-byte loads, and the 80-byte row stride
+// puts the rows of eight consecutive phases on distinct 16-byte bank groups.
+constexpr int kSincRow = 40;
+template <class W>
+__device__ __forceinline__ uint32_t sinc_gather_pm(const W *win, int base, int sn, Bracket b, const int16_t *tab_pm) {
+    if (b.idx < 0) return 0u;
+    if (b.idx >= -kSincFirst && b.idx <= sn - (kSincTaps + kSincFirst)) {
+        const uint4 *c4 = reinterpret_cast<const uint4 *>(tab_pm + (b.wq >> 7) * kSincRow);
+        const W *x = win + (b.idx + kSincFirst - base);
+        // the int32 half sums of sinc_gather (same bound, same exact integer result)
+        int ar0 = 0, ai0 = 0, ar1 = 0, ai1 = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint4 u = c4[q];
+            const uint32_t wd[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int t = 8 * q + e;                  // tap 2k in the low half of word k
+                const int ct = (e & 1) ? ((int)wd[e >> 1] >> 16) : (int)(int16_t)(wd[e >> 1] & 0xffffu);
+                const W v = x[t];
+                if (t < kSincTaps / 2) {
+                    ar0 += ct * re_of(v);
+                    ai0 += ct * im_of(v);
+                } else {
+                    ar1 += ct * re_of(v);
+                    ai1 += ct * im_of(v);
+                }
+            }
+        }
+        const long long ar = (long long)ar0 + ar1, ai = (long long)ai0 + ai1;
+        return pack16((int)sat16ll((ar + (1 << 14)) >> 15), (int)sat16ll((ai + (1 << 14)) >> 15));
+    }
+    const W va = win[b.idx - base], vb = win[b.idx + 1 - base];
+    const int ar = re_of(va), ai = im_of(va), br = re_of(vb), bi = im_of(vb);
+    return pack16(sat16(ar + (((br - ar) * b.wq) >> 15)), sat16(ai + (((bi - ai) * b.wq) >> 15)));
+}
+
 // apply_fixed (silicon_emulator.py:60-71).  F32PROD: the product (b-a)*wq rounded to float32, as in
 // pass 1 where the emulator's quantised signal is complex64.
 template <bool F32PROD, class W>
@@ -255,7 +293,7 @@ struct P1Pulse {
 
 constexpr size_t P1_SMEM_TILE = (size_t)P1_BINS * (P1_SLOTS + 1) * 4;
 constexpr size_t P1_SMEM_WIN = (size_t)P1_WARPS * P1_WMAX * 8;   // int32 I/Q pairs
-constexpr size_t p1_smem(bool sinc) { return P1_SMEM_TILE + P1_SMEM_WIN + (sinc ? 2 * 256 * kSincTaps : 0); }
+constexpr size_t p1_smem(bool sinc) { return P1_SMEM_TILE + P1_SMEM_WIN + (sinc ? 2 * 256 * kSincRow : 0); }
 
 template <bool SINC>
 __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
@@ -268,9 +306,8 @@ __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
     const int j0 = blockIdx.y * P1_BINS;
     const int n = a.n;
     if (SINC) {
-        const uint32_t *src = reinterpret_cast<const uint32_t *>(a.sinc);
-        uint32_t *dst = reinterpret_cast<uint32_t *>(tab);
-        for (int i = tid; i < 256 * kSincTaps / 2; i += blockDim.x) dst[i] = src[i];
+        // [tap][phase] in global memory -> phase-major rows of kSincRow in shared memory
+        for (int i = tid; i < 256 * kSincTaps; i += blockDim.x) tab[(i & 255) * kSincRow + (i >> 8)] = a.sinc[i];
     }
     __shared__ P1Pulse prm[P1_SLOTS];
     if (tid < P1_SLOTS) {
@@ -366,7 +403,7 @@ __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
             uint32_t out = 0u;
             if (j0 + jj < n && br[t].idx >= 0) {
                 if (fits) {
-                    out = SINC ? sinc_gather(w, wlo, n, br[t], tab)
+                    out = SINC ? sinc_gather_pm(w, wlo, n, br[t], tab)
                                : (a.cubic ? cubic_gather(w, wlo, n, br[t]) : lerp_gather<true>(w, wlo, br[t]));
                 } else {
                     // Window wider than the staging buffer: gather straight from global memory.
@@ -383,7 +420,7 @@ __global__ void __launch_bounds__(256, 4) k_fx_pass1(Pass1Args a) {
                             tmp[u] = a.sig_iq[off];
                         }
                     }
-                    out = SINC ? sinc_gather(tmp, base, n, br[t], tab)
+                    out = SINC ? sinc_gather_pm(tmp, base, n, br[t], tab)
                                : (a.cubic ? cubic_gather(tmp, base, n, br[t]) : lerp_gather<true>(tmp, base, br[t]));
                 }
             }
