@@ -254,8 +254,17 @@ __device__ __forceinline__ uint32_t cubic_gather(const W *win, int base, int sn,
 __global__ void k_q0max(const float4 *__restrict__ sig4, long long n4, const float *__restrict__ tail,
                         int ntail, uint32_t *__restrict__ out_bits) {
     float mx = 0.0f;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4;
-         i += (long long)gridDim.x * blockDim.x) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n4; i += 4 * stride) {      // four independent loads in flight
+        float4 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = __ldcs(sig4 + i + u * stride);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v[u].x), fabsf(v[u].y)), fmaxf(fabsf(v[u].z), fabsf(v[u].w))));
+    }
+    for (; i < n4; i += stride) {
         const float4 v = __ldcs(sig4 + i);
         mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
     }
@@ -720,9 +729,11 @@ __device__ __forceinline__ uint16_t detect_one(uint32_t v, int sh, int fused) {
     const int ps = fused ? 0 : sh;
     const int r = lo16(v) >> ps, i = hi16(v) >> ps;          // an arithmetic shift keeps int16 range
     const unsigned p = (unsigned)(r * r) + (unsigned)(i * i);
+    // p < 2^31 rounds to 24 bits in float, so the estimate is within 0.0014 of sqrt(p) and its truncation
+    // within one of floor(sqrt(p)): one correction each way makes q exact
     unsigned q = (unsigned)sqrtf((float)p);
-    while (q * q > p) --q;
-    while ((q + 1) * (q + 1) <= p) ++q;
+    q -= (q * q > p) ? 1u : 0u;
+    q += ((q + 1) * (q + 1) <= p) ? 1u : 0u;
     if (fused) q >>= sh;
     return (uint16_t)min(q, 65535u);
 }
