@@ -128,7 +128,7 @@ template <class W>
 __device__ __forceinline__ uint32_t sinc_gather(const W *win, int base, int sn, Bracket b, const int16_t *tab) {
     if (b.idx < 0) return 0u;
     if (b.idx >= -kSincFirst && b.idx <= sn - (kSincTaps + kSincFirst)) {
-        const int16_t *c = tab + (b.wq >> 7);           // table stored [tap][phase]: phases spread over banks
+        const int16_t *c = tab + (b.wq >> 7);           // table stored [tap][phase] (the global layout)
         const W *x = win + (b.idx + kSincFirst - base);
         // Two int32 half sums (taps 0-15, 16-31): the table is checked on upload to have
         // sum |tap| <= 65535 over each half of every phase, so |half sum| <= 32768 * 65535 < 2^31.
