@@ -55,7 +55,7 @@ def test_tile_values_checked(torch_cuda):
     for tile in ((32, 32), (16, 16)):
         with engine.FloatPlan(600, 900, tile=tile) as plan:
             plan.set_tables(tb)
-            out.append(plan.form(sc.signal, detect="complex").cpu().numpy())
+            out.append(np.asarray(plan.form(sc.signal, detect="complex")))
     assert np.array_equal(out[0], out[1])
 
 
