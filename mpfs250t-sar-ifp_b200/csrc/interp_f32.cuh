@@ -145,43 +145,47 @@ __device__ __forceinline__ void mirror_frac(Frac &fr) {
     fr.rev = 1;
 }
 
-// Float sinc table: 256 phases x 32 taps / 32768, one phase per row of kTabStride floats.  A lane reads
-// its phase's taps four at a time (16-byte loads); the 36-float stride puts the rows of 8 consecutive
-// phases on distinct 4-bank groups, so a warp's 32 phases cost 4 wavefronts per load, the minimum.
-constexpr int kTabStride = 36;
-constexpr int kTabFloats = 256 * kTabStride;
+// Float sinc table: the Q15 taps as int16, 256 phases x 32 taps, one phase per row of kTabRow int16 (taps
+// 0..31, then padding).  A lane reads its phase's taps eight at a time (four 16-byte loads; half the
+// shared-memory wavefronts of a float table, whose random-phase loads conflict the same way).
+constexpr int kTabRow = 40;
+constexpr int kTabShorts = 256 * kTabRow;
 
-// lerp or float sinc of complex64 samples `src` (indexed from `base`) at bracket (j, frac); the sinc
-// sums the taps in natural order (t = 0..31) with fused multiply-adds
+// exact float of a sign-extended int16 without the conversion unit: the bit pattern of 1.5 * 2^23 plus
+// v is the float 1.5 * 2^23 + v for |v| < 2^22
+__device__ __forceinline__ float s16f(int v) { return __int_as_float(0x4B400000 + v) - 12582912.0f; }
+
+// lerp or float sinc of complex64 samples `src` (indexed from `base`) at bracket (j, frac).  The sinc sums
+// the taps in natural order (t = 0..31) with fused multiply-adds on the integer tap values and scales the
+// sums by 2^-15 at the end: every partial sum is exactly 2^15 times the one a table of tap / 32768 gives
+// (scaling by a power of two commutes with rounding), so the result is the same float.
 template <bool SINC>
 __device__ __forceinline__ float2 gather_f32(const float2 *src, int base, int sn, int j, Frac fr,
-                                             const float *tab) {
+                                             const int16_t *tab) {
     if (j < 0) return make_float2(0.f, 0.f);
     const float frac = fr.f;
     if (SINC && j >= 15 && j <= sn - 17) {
-        const float4 *c4 = reinterpret_cast<const float4 *>(tab + fr.ph * kTabStride);
+        const uint4 *c4 = reinterpret_cast<const uint4 *>(tab + fr.ph * kTabRow);
         const float2 *x = src + (j - 15 - base);
         float ar = 0.f, ai = 0.f;
-        if (!fr.rev) {
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const float4 c = c4[q];
-                ar = fmaf(c.x, x[4 * q].x, ar);     ai = fmaf(c.x, x[4 * q].y, ai);
-                ar = fmaf(c.y, x[4 * q + 1].x, ar); ai = fmaf(c.y, x[4 * q + 1].y, ai);
-                ar = fmaf(c.z, x[4 * q + 2].x, ar); ai = fmaf(c.z, x[4 * q + 2].y, ai);
-                ar = fmaf(c.w, x[4 * q + 3].x, ar); ai = fmaf(c.w, x[4 * q + 3].y, ai);
-            }
-        } else {                                          // descending axis: tap 31 - t at sample t
+        for (int q = 0; q < 4; ++q) {
+            // taps 8g .. 8g+7 of group g (tap 2k in the low half of word k); descending axis: tap 31 - t
+            // at sample t, so sample group q takes tap group 3 - q in reverse
+            const uint4 u = c4[fr.rev ? 3 - q : q];
+            const uint32_t wd[4] = {u.x, u.y, u.z, u.w};
+            float c[8];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const float4 c = c4[7 - q];
-                ar = fmaf(c.w, x[4 * q].x, ar);     ai = fmaf(c.w, x[4 * q].y, ai);
-                ar = fmaf(c.z, x[4 * q + 1].x, ar); ai = fmaf(c.z, x[4 * q + 1].y, ai);
-                ar = fmaf(c.y, x[4 * q + 2].x, ar); ai = fmaf(c.y, x[4 * q + 2].y, ai);
-                ar = fmaf(c.x, x[4 * q + 3].x, ar); ai = fmaf(c.x, x[4 * q + 3].y, ai);
+            for (int e = 0; e < 8; ++e)
+                c[e] = s16f((e & 1) ? ((int)wd[e >> 1] >> 16) : ((int)(wd[e >> 1] << 16) >> 16));
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const float ce = fr.rev ? c[7 - e] : c[e];
+                ar = fmaf(ce, x[8 * q + e].x, ar);
+                ai = fmaf(ce, x[8 * q + e].y, ai);
             }
         }
-        return make_float2(ar, ai);
+        return make_float2(ar * (1.0f / 32768.0f), ai * (1.0f / 32768.0f));
     }
     const float2 a = src[j - base], b = src[j + 1 - base];
     return make_float2(fmaf(frac, b.x - a.x, a.x), fmaf(frac, b.y - a.y, a.y));

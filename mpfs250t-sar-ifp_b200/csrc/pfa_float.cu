@@ -46,14 +46,14 @@ constexpr int fl_min_ctas(int L, int E) {
 // F1_BINS consecutive bins cover at most F1_BINS + 1 source intervals; a wider window (not produced by
 // prepare_tables) falls back to gathering from global memory.
 constexpr int F1_SLOTS = 32, F1_WARPS = 8, F1_WMAX = 144;
-// range bins per CTA: the sinc variant takes a narrower tile so three CTAs (with the 36 KB table) fit an SM
+// range bins per CTA: the sinc variant takes a narrower tile so three CTAs (with the 20 KB table) fit an SM
 constexpr int f1_bins(bool sinc) { return sinc ? 64 : 128; }
 
 struct FPass1Args {
     const float2 *sig;
     const double *f0, *df, *flast, *pr, *kr_grid;
     const int32_t *order;
-    const float *tabf;
+    const int16_t *tabq;
     const float *theta;     // per-pulse phase correction exp(-j theta_i) (autofocus), or nullptr
     float2 *p1;
     int m, n, mpad;
@@ -68,7 +68,7 @@ struct F1Pulse {
 };
 
 constexpr size_t f1_smem(bool sinc) {
-    return (size_t)f1_bins(sinc) * (F1_SLOTS + 1) * 8 + (size_t)F1_WARPS * 2 * F1_WMAX * 8 + (sinc ? kTabFloats * 4 : 0);
+    return (size_t)f1_bins(sinc) * (F1_SLOTS + 1) * 8 + (size_t)F1_WARPS * 2 * F1_WMAX * 8 + (sinc ? kTabShorts * 2 : 0);
 }
 
 template <bool SINC>
@@ -78,16 +78,16 @@ __global__ void __launch_bounds__(256, SINC ? 3 : 4) k_fl_pass1(FPass1Args a) {
     constexpr size_t TILE_BYTES = (size_t)F1_BINS * (F1_SLOTS + 1) * 8;
     float2(*tile)[F1_SLOTS + 1] = reinterpret_cast<float2(*)[F1_SLOTS + 1]>(smem);
     float2(*win)[2][F1_WMAX] = reinterpret_cast<float2(*)[2][F1_WMAX]>(smem + TILE_BYTES);
-    float *tab = reinterpret_cast<float *>(smem + TILE_BYTES + (size_t)F1_WARPS * 2 * F1_WMAX * 8);
+    int16_t *tab = reinterpret_cast<int16_t *>(smem + TILE_BYTES + (size_t)F1_WARPS * 2 * F1_WMAX * 8);
     __shared__ F1Pulse prm[F1_SLOTS];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r0 = blockIdx.x * F1_SLOTS, j0 = blockIdx.y * F1_BINS;
     const int n = a.n;
     if (SINC) {
-        const float4 *src = reinterpret_cast<const float4 *>(a.tabf);
-        float4 *dst = reinterpret_cast<float4 *>(tab);
+        const uint4 *src = reinterpret_cast<const uint4 *>(a.tabq);
+        uint4 *dst = reinterpret_cast<uint4 *>(tab);
 #pragma unroll
-        for (int i = 0; i < kTabFloats / 4 / 256; ++i) dst[tid + 256 * i] = __ldg(src + tid + 256 * i);
+        for (int i = 0; i < kTabShorts / 8 / 256; ++i) dst[tid + 256 * i] = __ldg(src + tid + 256 * i);
     }
     if (tid < F1_SLOTS) {
         F1Pulse p{};
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(256, SINC ? 3 : 4) k_fl_pass1(FPass1Args a) {
 struct FPass2Args {
     const float2 *p1;
     const double *tan_s, *kr_grid, *kc_grid, *ham_m, *ham_n;
-    const float *tabf;
+    const int16_t *tabq;
     const float2 *tw;
     float2 *y1t;          // [m2][npad] cross-FFT output, transposed: row = cross bin, col = range bin
     int m, n, mpad, npad, centred, window, inverse;
@@ -260,7 +260,7 @@ k_fl_pass2_fft(FPass2Args a) {
     const size_t regA = (max((size_t)8 * m, (size_t)8 * F::xbuf_elems()) + 15) & ~(size_t)15;
     float2 *row = reinterpret_cast<float2 *>(smem);
     float2 *xbuf = reinterpret_cast<float2 *>(smem);
-    float *tab = reinterpret_cast<float *>(smem + regA);
+    int16_t *tab = reinterpret_cast<int16_t *>(smem + regA);
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     const int tid = threadIdx.x;
@@ -274,7 +274,7 @@ k_fl_pass2_fft(FPass2Args a) {
         const int nchunk = (m + 1) >> 1;                      // 16-byte chunks (the pad covers odd m)
         for (int c = tid; c < nchunk; c += T) cp_async16(row + 2 * c, src + 2 * c);
         if (SINC)
-            for (int c = tid; c < kTabFloats / 4; c += T) cp_async16(tab + 4 * c, a.tabf + 4 * c);
+            for (int c = tid; c < kTabShorts / 8; c += T) cp_async16(tab + 8 * c, a.tabq + 8 * c);
         cp_async_commit();
     }
     const double krj = a.kr_grid[j];
@@ -650,10 +650,10 @@ struct Cfg {
 template <int L, int E, bool SINC>
 cudaError_t launch_pass2(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, E>;
-    FPass2Args p{d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabf,
+    FPass2Args p{d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabq,
                  d.twm, d.y1, d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0};
     size_t regA = (std::max((size_t)8 * d.m, (size_t)8 * F::xbuf_elems()) + 15) & ~(size_t)15;
-    size_t sm = regA + (SINC ? kTabFloats * 4 : 0);
+    size_t sm = regA + (SINC ? kTabShorts * 2 : 0);
     auto fn = k_fl_pass2_fft<L, E, SINC>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
@@ -767,7 +767,7 @@ cudaError_t float_alloc(FloatDev &d, int m, int n) {
     TRY(dal(&d.f0, m)); TRY(dal(&d.df, m)); TRY(dal(&d.flast, m)); TRY(dal(&d.pr, m)); TRY(dal(&d.tan_s, m)); TRY(dal(&d.order, m));
     TRY(dal(&d.kr, n)); TRY(dal(&d.kc, m)); TRY(dal(&d.ham_m64, m)); TRY(dal(&d.ham_n64, n));
     TRY(dal(&d.twm, d.m2)); TRY(dal(&d.twn, d.n2));
-    TRY(dal(&d.tabf, kTabFloats));
+    TRY(dal(&d.tabq, kTabShorts));
     TRY(dal(&d.p1, (size_t)n * d.mpad)); TRY(dal(&d.y1, (size_t)d.npad * d.m2));
 #undef TRY
     return cudaSuccess;
@@ -775,7 +775,7 @@ cudaError_t float_alloc(FloatDev &d, int m, int n) {
 
 void float_free(FloatDev &d) {
     dfr(d.f0); dfr(d.df); dfr(d.flast); dfr(d.pr); dfr(d.tan_s); dfr(d.order); dfr(d.kr); dfr(d.kc); dfr(d.ham_m64);
-    dfr(d.ham_n64); dfr(d.twm); dfr(d.twn); dfr(d.tabf); dfr(d.p1); dfr(d.y1);
+    dfr(d.ham_n64); dfr(d.twm); dfr(d.twn); dfr(d.tabq); dfr(d.p1); dfr(d.y1);
     dfr(d.af_zadj); dfr(d.af_acc); dfr(d.af_dacc);
     mixed_free(d);
 }
@@ -786,7 +786,7 @@ cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int dete
     pf.count = 0;
     cudaError_t e = pf.mark(st, "start");
     if (e != cudaSuccess) return e;
-    FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabf, nullptr, d.p1, d.m, d.n, d.mpad};
+    FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabq, nullptr, d.p1, d.m, d.n, d.mpad};
     dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + f1_bins(d.range_sinc) - 1) / f1_bins(d.range_sinc));
     if (d.range_sinc) {
         e = cudaFuncSetAttribute(k_fl_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1_smem(true));
@@ -884,7 +884,7 @@ cudaError_t autofocus_grad(const FloatDev &d0, const float2 *sig, const float *t
     d.sgn = -1;
     if ((e = cudaMemsetAsync(d.af_acc, 0, 2 * sizeof(double), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(d.af_dacc, 0, sizeof(float) * d.mpad, st)) != cudaSuccess) return e;
-    FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabf, theta, d.p1, d.m, d.n, d.mpad};
+    FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabq, theta, d.p1, d.m, d.n, d.mpad};
     dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + f1_bins(false) - 1) / f1_bins(false));
     e = cudaFuncSetAttribute(k_fl_pass1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1_smem(false));
     if (e != cudaSuccess) return e;
@@ -945,9 +945,9 @@ pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *job) {
     std::vector<float2> twm, twn;
     pfa::full_twiddles(d.m2, twm);
     pfa::full_twiddles(d.n2, twn);
-    std::vector<float> tabf(pfa::kTabFloats, 0.0f);
+    std::vector<int16_t> tabq(pfa::kTabShorts, 0);
     const int16_t *tq = pfa::builtin_sinc_table();
-    for (int i = 0; i < 256 * 32; ++i) tabf[(i >> 5) * pfa::kTabStride + (i & 31)] = (float)tq[i] / 32768.0f;   // [phase][tap], padded rows
+    for (int i = 0; i < 256 * 32; ++i) tabq[(i >> 5) * pfa::kTabRow + (i & 31)] = tq[i];   // [phase][tap], padded rows
     cudaError_t e;
 #define CPY(dst, src, cnt) do { e = cudaMemcpy(dst, src, sizeof(*(dst)) * (cnt), cudaMemcpyHostToDevice); \
         if (e != cudaSuccess) return fcuda(p, e, "float job upload"); } while (0)
@@ -955,7 +955,7 @@ pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *job) {
     CPY(d.order, job->order, m); CPY(d.kr, job->kr_grid, n); CPY(d.kc, job->kc_grid, m);
     if (d.window) { CPY(d.ham_m64, job->ham_m, m); CPY(d.ham_n64, job->ham_n, n); }
     CPY(d.twm, twm.data(), d.m2); CPY(d.twn, twn.data(), d.n2);
-    CPY(d.tabf, tabf.data(), pfa::kTabFloats);
+    CPY(d.tabq, tabq.data(), pfa::kTabShorts);
 #undef CPY
     p->job_ready = true;
     return PFA_OK;

@@ -41,7 +41,7 @@ struct FloatDev {
     double *ham_m64 = nullptr, *ham_n64 = nullptr;
     int32_t *order = nullptr;
     float2 *twm = nullptr, *twn = nullptr;      // stage-contiguous twiddles for m2 and n2
-    float *tabf = nullptr;                      // sinc table / 32768, [phase][tap] rows of 36 floats
+    int16_t *tabq = nullptr;                    // sinc table (Q15 taps), [phase][tap] rows of 40 int16
     int window = 1;
     float2 *p1 = nullptr;              // [n][mpad] pass-1 output (range-bin rows, sorted pulses)
     float2 *y1 = nullptr;              // [m2][npad] cross FFT output, transposed (cross-bin rows)

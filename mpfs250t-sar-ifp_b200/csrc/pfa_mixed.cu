@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(Geo<L>::THREADS, 1) k_mx_fft2(MxFft2Args a) {
 struct MxPass2Args {
     const float2 *p1;
     const double *tan_s, *kr_grid, *kc_grid, *ham_m, *ham_n;
-    const float *tabf;
+    const int16_t *tabq;
     const float2 *tw;
     const uint4 *fn2, *f128;
     float2 *y1t;
@@ -229,8 +229,8 @@ __global__ void __cluster_dims__(kMxCT, 1, 1) __launch_bounds__(Geo<L>::THREADS,
     unsigned char *fn2 = smem;
     unsigned char *b2 = smem + G::FN2_BYTES;                 // stage-2 operand, then the exchange line
     float2 *row = reinterpret_cast<float2 *>(b2 + G::B2_BYTES);
-    float *tab = reinterpret_cast<float *>(b2 + G::B2_BYTES + row_bytes);
-    float *red = tab + (SINC ? kTabFloats : 0);
+    int16_t *tab = reinterpret_cast<int16_t *>(b2 + G::B2_BYTES + row_bytes);
+    float *red = reinterpret_cast<float *>(b2 + G::B2_BYTES + row_bytes + (SINC ? 2 * kTabShorts : 0));
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tbase;
     namespace cg = cooperative_groups;
@@ -245,7 +245,8 @@ __global__ void __cluster_dims__(kMxCT, 1, 1) __launch_bounds__(Geo<L>::THREADS,
     }
     F::load_fn2(a.fn2, fn2, tid);
     if (SINC)
-        for (int i = tid; i < kTabFloats; i += T) tab[i] = __ldg(a.tabf + i);
+        for (int i = tid; i < kTabShorts / 8; i += T)
+            reinterpret_cast<uint4 *>(tab)[i] = __ldg(reinterpret_cast<const uint4 *>(a.tabq) + i);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -431,7 +432,7 @@ size_t fft2_smem() {
 template <int L, bool SINC>
 size_t pass2_smem(int m) {
     return std::max(kMxMinSmem, (size_t)Geo<L>::FN2_BYTES + Geo<L>::B2_BYTES + (((size_t)8 * m + 15) & ~(size_t)15) +
-                                    (SINC ? kTabFloats * 4 : 0) + 64 * 4);
+                                    (SINC ? kTabShorts * 2 : 0) + 64 * 4);
 }
 
 template <int L>
@@ -449,7 +450,7 @@ cudaError_t launch_mx_fft2(const FloatDev &d, void *out, int detect, float scale
 template <int L, bool SINC>
 cudaError_t launch_mx_pass2(const FloatDev &d, cudaStream_t st) {
     const int ngroups = d.npad / kMxCT;
-    MxPass2Args p{d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabf, d.twm, d.mx_fn2m, d.mx_f128, d.y1,
+    MxPass2Args p{d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabq, d.twm, d.mx_fn2m, d.mx_f128, d.y1,
                   d.mx_err, d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0, ngroups};
     const size_t sm = pass2_smem<L, SINC>(d.m);
     auto fn = k_mx_pass2<L, SINC>;
