@@ -232,6 +232,13 @@ __global__ void __launch_bounds__(256, SINC ? 3 : 4) k_fl_pass1(FPass1Args a) {
     }
 }
 
+// packed pass-2 bracket (written by the lerp pass 2 for the autofocus adjoint): bit 31 = outside the span, bits 17..30 = lower index, bits 0..16 = weight
+__device__ __forceinline__ uint32_t pack_br(int dead, int lowi, float f) {
+    const uint32_t q = (uint32_t)fminf(fmaxf(rintf(f * 131071.f), 0.f), 131071.f);
+    return ((uint32_t)dead << 31) | ((uint32_t)lowi << 17) | q;
+}
+__device__ __forceinline__ int br_low(uint32_t p) { return (int)((p >> 17) & 0x3fffu); }
+
 // ------------------------------------------------------------------------------------------ K2f
 struct FPass2Args {
     const float2 *p1;
@@ -239,6 +246,7 @@ struct FPass2Args {
     const int16_t *tabq;
     const float2 *tw;
     float2 *y1t;          // [m2][npad] cross-FFT output, transposed: row = cross bin, col = range bin
+    uint32_t *pk_out;     // lerp: packed brackets [j][k] for the autofocus adjoint, or nullptr
     int m, n, mpad, npad, centred, window, inverse;
 };
 
@@ -250,7 +258,9 @@ struct FPass2Args {
 constexpr int kCT = 4;
 static_assert(8 % kCT == 0, "npad (a multiple of 8) must hold whole clusters");
 
-template <int L, int E, bool SINC>
+// PK: also store the packed brackets for the autofocus adjoint (lerp only; a separate instantiation so
+// that the frame's pass 2 carries no extra register pressure)
+template <int L, int E, bool SINC, bool PK = false>
 __global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, fl_min_ctas(L, E))
 k_fl_pass2_fft(FPass2Args a) {
     using F = F32Fft<L, E>;
@@ -310,6 +320,12 @@ k_fl_pass2_fft(FPass2Args a) {
                 if (!asc) { lowi = m - 2 - ja[c]; mirror_frac(fr[c]); }
                 bl[u] = lowi | (fr[c].ph << 16) | (fr[c].rev << 24);
                 bf[u] = fr[c].f;
+            }
+            if constexpr (PK && !SINC) {
+                // the adjoint's brackets (ascending sources: the autofocus plan has KR > 0)
+                if (ok[c])
+                    a.pk_out[(size_t)j * m + tid + T * u] =
+                        ja[c] >= 0 ? pack_br(0, ja[c], fr[c].f) : pack_br(1, q[c] < lo_v ? 0 : m - 2, 0.f);
             }
         }
     }
@@ -506,18 +522,13 @@ k_af_range_adjoint(AfRangeArgs a) {
 struct AfCrossArgs {
     const float2 *zadj_t;   // [n][m2]
     const float2 *p1;       // [n][mpad] forward pass-1 output (phase corrected)
-    const double *tan_s, *kr_grid, *kc_grid, *ham_m, *ham_n;
+    const uint32_t *pk;     // [n][m] packed brackets of the forward pass 2
+    const double *ham_m, *ham_n;
     const float2 *tw;       // cross twiddles (m2)
     float *dacc;            // [mpad] per-slot Im sum conj(g_p1) p1
     int m, n, mpad, window;
 };
 
-// packed pass-2 bracket: bit 31 = outside the span, bits 17..30 = lower index, bits 0..16 = weight
-__device__ __forceinline__ uint32_t pack_br(int dead, int lowi, float f) {
-    const uint32_t q = (uint32_t)fminf(fmaxf(rintf(f * 131071.f), 0.f), 131071.f);
-    return ((uint32_t)dead << 31) | ((uint32_t)lowi << 17) | q;
-}
-__device__ __forceinline__ int br_low(uint32_t p) { return (int)((p >> 17) & 0x3fffu); }
 // Shared-memory positions of bracket k and of W . F^H g at cross index k in the cross adjoint.  Its
 // segmented reduction has lane t walk indices near 16 t; XOR-ing the low four index bits with bits of
 // the group index (a permutation inside each aligned group of 16) spreads those lanes over the banks
@@ -536,26 +547,10 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
     const int tid = threadIdx.x;
     const int j = blockIdx.x;                         // range bin (< n)
     const int m = a.m;
-    // forward pass-2 brackets of this range bin (ascending source axis: KR[j] > 0)
-    const double krj = a.kr_grid[j];
-    const double lo_v = krj * a.tan_s[0], hi_v = krj * a.tan_s[m - 1];
-    auto xa = [&](int t) { return krj * __ldg(a.tan_s + t); };
-    const double inv_span = (double)(m - 1) / (hi_v - lo_v);
-    constexpr int CH = 2;
-    for (int k0 = tid; k0 < m; k0 += CH * T) {
-        double q[CH];
-        bool ok[CH];
-#pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            ok[c] = k0 + c * T < m;
-            q[c] = ok[c] ? __ldg(a.kc_grid + k0 + c * T) : 0.0;
-        }
-        int ja[CH];
-        Frac fr[CH];
-        interp_brackets<false, CH>(xa, m, lo_v, hi_v, inv_span, q, ok, ja, fr);
-#pragma unroll
-        for (int c = 0; c < CH; ++c)
-            if (ok[c]) pk[pk_at(k0 + c * T)] = ja[c] >= 0 ? pack_br(0, ja[c], fr[c].f) : pack_br(1, q[c] < lo_v ? 0 : m - 2, 0.f);
+    // the forward pass-2 brackets of this range bin (stored by the forward pass 2 of this gradient)
+    {
+        const uint32_t *src = a.pk + (size_t)j * m;
+        for (int k = tid; k < m; k += T) pk[pk_at(k)] = __ldcs(src + k);
     }
     // adjoint of the cross FFT
     const float2 *row = a.zadj_t + (size_t)j * N;
@@ -651,10 +646,13 @@ template <int L, int E, bool SINC>
 cudaError_t launch_pass2(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, E>;
     FPass2Args p{d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabq,
-                 d.twm, d.y1, d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0};
+                 d.twm, d.y1, d.pk_out, d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0};
     size_t regA = (std::max((size_t)8 * d.m, (size_t)8 * F::xbuf_elems()) + 15) & ~(size_t)15;
     size_t sm = regA + (SINC ? kTabShorts * 2 : 0);
     auto fn = k_fl_pass2_fft<L, E, SINC>;
+    if constexpr (!SINC) {
+        if (d.pk_out) fn = k_fl_pass2_fft<L, E, false, true>;
+    }
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     fn<<<d.npad, (1 << L) / E, sm, st>>>(p);
@@ -776,7 +774,7 @@ cudaError_t float_alloc(FloatDev &d, int m, int n) {
 void float_free(FloatDev &d) {
     dfr(d.f0); dfr(d.df); dfr(d.flast); dfr(d.pr); dfr(d.tan_s); dfr(d.order); dfr(d.kr); dfr(d.kc); dfr(d.ham_m64);
     dfr(d.ham_n64); dfr(d.twm); dfr(d.twn); dfr(d.tabq); dfr(d.p1); dfr(d.y1);
-    dfr(d.af_zadj); dfr(d.af_acc); dfr(d.af_dacc);
+    dfr(d.af_zadj); dfr(d.af_acc); dfr(d.af_dacc); dfr(d.af_pk);
     mixed_free(d);
 }
 
@@ -830,7 +828,7 @@ cudaError_t launch_af_range(const FloatDev &d, cudaStream_t st) {
 template <int L>
 cudaError_t launch_af_cross(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, Cfg<L>::E>;
-    AfCrossArgs p{d.af_zadj, d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.twm, d.af_dacc, d.m, d.n, d.mpad, d.window};
+    AfCrossArgs p{d.af_zadj, d.p1, d.af_pk, d.ham_m64, d.ham_n64, d.twm, d.af_dacc, d.m, d.n, d.mpad, d.window};
     const size_t sm = (size_t)8 * F::xbuf_elems() + (size_t)4 * ((d.m + 15) & ~15);   // pk: whole groups of 16
     auto fn = k_af_cross_adjoint<L, Cfg<L>::E>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -882,6 +880,7 @@ cudaError_t autofocus_grad(const FloatDev &d0, const float2 *sig, const float *t
     FloatDev d = d0;
     d.layout = PFA_LAYOUT_NATURAL;      // |z| (so E) does not depend on the centring
     d.sgn = -1;
+    d.pk_out = d.af_pk;                 // the forward pass 2 keeps its brackets for the cross adjoint
     if ((e = cudaMemsetAsync(d.af_acc, 0, 2 * sizeof(double), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(d.af_dacc, 0, sizeof(float) * d.mpad, st)) != cudaSuccess) return e;
     FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabq, theta, d.p1, d.m, d.n, d.mpad};
@@ -1051,8 +1050,9 @@ pfa_status pfa_autofocus_grad(pfa_plan *p, const float *sig_dev, const float *th
     cudaError_t e;
     if (!d.af_zadj) {
         if ((e = pfa::dal(&d.af_zadj, (size_t)d.n * d.m2)) != cudaSuccess ||
-            (e = pfa::dal(&d.af_acc, 2)) != cudaSuccess || (e = pfa::dal(&d.af_dacc, d.mpad)) != cudaSuccess) {
-            pfa::dfr(d.af_zadj); pfa::dfr(d.af_acc); pfa::dfr(d.af_dacc);
+            (e = pfa::dal(&d.af_acc, 2)) != cudaSuccess || (e = pfa::dal(&d.af_dacc, d.mpad)) != cudaSuccess ||
+            (e = pfa::dal(&d.af_pk, (size_t)d.n * d.m)) != cudaSuccess) {
+            pfa::dfr(d.af_zadj); pfa::dfr(d.af_acc); pfa::dfr(d.af_dacc); pfa::dfr(d.af_pk);
             return fcuda(p, e, "autofocus workspace");
         }
     }

@@ -50,6 +50,8 @@ struct FloatDev {
     float2 *af_zadj = nullptr;         // [n][m2] autofocus: adjoint of the range FFT (range-bin rows)
     double *af_acc = nullptr;          // [2] sum I, sum I log I
     float *af_dacc = nullptr;          // [mpad] per-slot gradient accumulators
+    uint32_t *af_pk = nullptr;         // [n][m] autofocus: packed pass-2 brackets of the forward pass
+    uint32_t *pk_out = nullptr;        // where the lerp pass 2 stores its packed brackets (or nullptr)
     // split-precision (mixed) mode: tensor-core FFTs for lines of 2048..8192 points
     int mixed = 0;
     uint4 *mx_f128 = nullptr;          // F_128 TMEM image [128 lanes][256 columns] of fp16 pairs
