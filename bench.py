@@ -26,6 +26,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -34,7 +35,7 @@ sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "mpfs250t-sar-ifp_b200"))
 
 METRIC = "ms per 8192^2 PFA frame (mixed vs FP32 at stated err vs FP64); autofocus grads/s"
-FPGA_FRAME_MS = {"centerfield_5634x4319": 14170.0, "ndsu_8167x8192": 15738.0}   # BASELINE.md (MPFS250T fabric)
+FPGA_FRAME_MS = {"centerfield_5634x4319": 14170.0, "ndsu_8167x8192": 15738.0}   # published MPFS250T fabric frame times
 
 WORKLOADS = {
     "centerfield_5634x4319": dict(mode="fixed", grid=8192, range_sinc=True, az_sinc=True, scene="centerfield_5634x4319",
@@ -67,11 +68,10 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_dev{device}.csv"
+        self.path = Path(tempfile.gettempdir()) / f"pfa_bench_clocks_dev{device}_{os.getpid()}.csv"
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],

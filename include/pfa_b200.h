@@ -168,13 +168,16 @@ pfa_status pfa_form_float_host_frames(pfa_plan *plan, const float *const *sig_ho
  * allocates; this mirrors that property rather than any one function).
  * Everything the frame needs besides the caller's signal and image -- the job vectors and the three
  * intermediate frames -- lives in one file-scope static __device__ array of 12.1 MB that every GPU
- * which loads the library holds until the process exits.  Limits: grid <= 1024, m <= grid, n <= grid,
- * otherwise PFA_ERR_TOO_LARGE.  job must carry ham_r, ham_c and twiddle (no host-side table building);
- * sinc_q15 may be NULL (built-in table).  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress, with that device current); make that first call before any stream capture.
- * All calls share the one array and it keeps the last call's contents: calls that overlap on the GPU
- * (different streams, threads or processes sharing a context) race and corrupt each other; serialise
- * them.  Calls no allocating routine: no cudaMalloc/cudaFree, no host heap. */
+ * which loads the library holds until the process exits.  Limits: grid <= 1024, otherwise
+ * PFA_ERR_TOO_LARGE; m or n > grid gives PFA_ERR_BAD_DIMS.  job must carry ham_r, ham_c and twiddle (no
+ * host-side table building); sinc_q15 may be NULL (built-in table).  The job vectors are copied to the
+ * device with cudaMemcpyAsync on `stream`: like any asynchronous copy from (possibly pinned) host memory,
+ * the job arrays and sinc_q15 must stay valid and unchanged until the stream has reached this call's work.
+ * Every call looks up the array's device address (cudaGetSymbolAddress, with that device current); the
+ * first call on a device also loads the library's device code there, so make that first call before any
+ * stream capture.  All calls share the one array and it keeps the last call's contents: calls that overlap
+ * on the GPU (different streams, threads or processes sharing a context) race and corrupt each other;
+ * serialise them.  Calls no allocating routine: no cudaMalloc/cudaFree, no host heap. */
 pfa_status pfa_form_fixed_noalloc(const pfa_config *cfg, const pfa_fixed_job *job, const float *sig_dev,
                                   uint16_t *img_dev, void *stream);
 

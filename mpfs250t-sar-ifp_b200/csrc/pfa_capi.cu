@@ -374,28 +374,37 @@ pfa_status pfa::run_host_frames(pfa_plan *p, const void *const *ins, void *const
         p->pipe_out_bytes = out_b;
     }
     cudaEvent_t *uploaded = p->pipe_ev, *computed = p->pipe_ev + 2, *downloaded = p->pipe_ev + 4;
+    // Once the first copy is enqueued, every return drains the three streams first: copies into and out of
+    // the caller's host buffers and the staging buffers must not outlive the call, and the next call's
+    // frames 0 and 1 reuse the staging buffers without waiting on this call's events.
+    auto drain = [p](pfa_status st) {
+        for (cudaStream_t s : {p->pipe_up, p->pipe_comp, p->pipe_down}) {
+            cudaError_t es = cudaStreamSynchronize(s);
+            if (es != cudaSuccess && st == PFA_OK) st = cuda_fail(p, es, "pipe sync");
+        }
+        return st;
+    };
     for (int k = 0; k < nframes; ++k) {
         const int b = k & 1;
         // upload k once frame k-2 no longer reads this staging buffer
-        if (k >= 2 && (e = cudaStreamWaitEvent(p->pipe_up, computed[b], 0)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+        if (k >= 2 && (e = cudaStreamWaitEvent(p->pipe_up, computed[b], 0)) != cudaSuccess) return drain(cuda_fail(p, e, "pipe"));
         if ((e = cudaMemcpyAsync(p->pipe_in[b], ins[k], in_b, cudaMemcpyHostToDevice, p->pipe_up)) != cudaSuccess)
-            return cuda_fail(p, e, "pipe h2d");
-        if ((e = cudaEventRecord(uploaded[b], p->pipe_up)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+            return drain(cuda_fail(p, e, "pipe h2d"));
+        if ((e = cudaEventRecord(uploaded[b], p->pipe_up)) != cudaSuccess) return drain(cuda_fail(p, e, "pipe"));
         // frame k after its upload, and after frame k-2's image left this output buffer
-        if ((e = cudaStreamWaitEvent(p->pipe_comp, uploaded[b], 0)) != cudaSuccess) return cuda_fail(p, e, "pipe");
-        if (k >= 2 && (e = cudaStreamWaitEvent(p->pipe_comp, downloaded[b], 0)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+        if ((e = cudaStreamWaitEvent(p->pipe_comp, uploaded[b], 0)) != cudaSuccess) return drain(cuda_fail(p, e, "pipe"));
+        if (k >= 2 && (e = cudaStreamWaitEvent(p->pipe_comp, downloaded[b], 0)) != cudaSuccess)
+            return drain(cuda_fail(p, e, "pipe"));
         pfa_status st = form(p, p->pipe_in[b], p->pipe_out[b], p->pipe_comp, arg);
-        if (st != PFA_OK) return st;
-        if ((e = cudaEventRecord(computed[b], p->pipe_comp)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+        if (st != PFA_OK) return drain(st);
+        if ((e = cudaEventRecord(computed[b], p->pipe_comp)) != cudaSuccess) return drain(cuda_fail(p, e, "pipe"));
         // download k
-        if ((e = cudaStreamWaitEvent(p->pipe_down, computed[b], 0)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+        if ((e = cudaStreamWaitEvent(p->pipe_down, computed[b], 0)) != cudaSuccess) return drain(cuda_fail(p, e, "pipe"));
         if ((e = cudaMemcpyAsync(outs[k], p->pipe_out[b], out_b, cudaMemcpyDeviceToHost, p->pipe_down)) != cudaSuccess)
-            return cuda_fail(p, e, "pipe d2h");
-        if ((e = cudaEventRecord(downloaded[b], p->pipe_down)) != cudaSuccess) return cuda_fail(p, e, "pipe");
+            return drain(cuda_fail(p, e, "pipe d2h"));
+        if ((e = cudaEventRecord(downloaded[b], p->pipe_down)) != cudaSuccess) return drain(cuda_fail(p, e, "pipe"));
     }
-    for (cudaStream_t s : {p->pipe_up, p->pipe_comp, p->pipe_down})
-        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(p, e, "pipe sync");
-    return PFA_OK;
+    return drain(PFA_OK);
 }
 
 extern "C" {

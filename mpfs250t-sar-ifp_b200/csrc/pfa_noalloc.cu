@@ -7,9 +7,14 @@
 // largest frame it accepts (grid 1024: 12.1 MB, held by every GPU that loads the library until exit).
 //
 // Host code must not pass the array's name to a kernel: on the host that name is only a stand-in
-// symbol, not a device address.  The device address is looked up once per device with
-// cudaGetSymbolAddress (that device current) on the first call and cached.  The same kernels as the
-// planned path (pfa_fixed.cu) run on a FixedDev view whose pointers point into the array.
+// symbol, not a device address.  Every call looks the device address up with cudaGetSymbolAddress (the
+// call's device current).  The first lookup on a device loads the module there; later ones are cheap and
+// never stale, also after a device reset reloaded the module.  The same kernels as the planned path
+// (pfa_fixed.cu) run on a FixedDev view whose pointers point into the array.
+//
+// The job vectors are copied host-to-device with cudaMemcpyAsync on the caller's stream.  From pinned
+// host memory those copies are truly asynchronous, so the job arrays (and sinc_q15) must stay valid and
+// unchanged until the stream has reached this call's work, the contract of any asynchronous copy.
 //
 // All calls share the array and it keeps the previous call's contents.  What must start at zero (the
 // reduction words) is cleared by every call; everything else is fully rewritten before it is read.
@@ -28,7 +33,6 @@ const int16_t *builtin_sinc_table();
 namespace {
 
 constexpr int kMaxGrid = 1024;
-constexpr int kMaxDevices = 64;
 
 constexpr size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
@@ -61,8 +65,6 @@ struct NoAllocLayout {
 
 // The scratch itself.  Only device code may name it directly; host code uses the looked-up address.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NoAllocLayout::total];
-
-void *g_scratch_addr[kMaxDevices] = {};
 
 // Derived job vectors: the pass-1 source scale f32(f32(2 pr) / f32(c)), the slot -> pulse order and the
 // stage-contiguous twiddle table (stage b at offset 2^b - 1, entry k = raw[k << (L-1-b)]).
@@ -107,7 +109,6 @@ extern "C" pfa_status pfa_form_fixed_noalloc(const pfa_config *cfg, const pfa_fi
     if (!job->f0 || !job->df || !job->pr || !job->tan_s || !job->inv_order || !job->kr_grid || !job->kc_grid ||
         !job->ham_r || !job->ham_c || !job->twiddle)
         return PFA_ERR_BAD_ARG;
-    if (reinterpret_cast<uintptr_t>(sig_dev) & 15) return PFA_ERR_BAD_ARG;
     // inv_order must be a permutation (it drives row indexing); checked with a stack bitmap
     uint32_t seen[kMaxGrid / 32] = {};
     for (int i = 0; i < c.m; ++i) {
@@ -115,7 +116,8 @@ extern "C" pfa_status pfa_form_fixed_noalloc(const pfa_config *cfg, const pfa_fi
         if (r < 0 || r >= c.m || (seen[r >> 5] >> (r & 31)) & 1u) return PFA_ERR_BAD_ARG;
         seen[r >> 5] |= 1u << (r & 31);
     }
-    if (c.device < 0 || c.device >= kMaxDevices) return PFA_ERR_NO_DEVICE;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || c.device < 0 || c.device >= ndev) return PFA_ERR_NO_DEVICE;
     int prev = -1;
     if (cudaGetDevice(&prev) != cudaSuccess) return PFA_ERR_NO_DEVICE;
     if (prev != c.device && cudaSetDevice(c.device) != cudaSuccess) return PFA_ERR_NO_DEVICE;
@@ -124,14 +126,11 @@ extern "C" pfa_status pfa_form_fixed_noalloc(const pfa_config *cfg, const pfa_fi
         ~Restore() { if (prev != dev) cudaSetDevice(prev); }
     } restore{prev, c.device};
 
-    // set-up, once per device: the device address of the static scratch
-    if (!g_scratch_addr[c.device]) {
-        void *addr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
-        if (e != cudaSuccess || !addr) return PFA_ERR_CUDA;
-        g_scratch_addr[c.device] = addr;
-    }
-    unsigned char *base = static_cast<unsigned char *>(g_scratch_addr[c.device]);
+    // set-up, on every call with the device current: the device address of the static scratch
+    void *addr = nullptr;
+    const cudaError_t ea = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (ea != cudaSuccess || !addr) return PFA_ERR_CUDA;
+    unsigned char *base = static_cast<unsigned char *>(addr);
     using Lt = NoAllocLayout;
     const int m = c.m, n = c.n, G = c.grid;
     int L = 0;

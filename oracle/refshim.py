@@ -7,8 +7,8 @@ package in ``sys.modules`` whose ``open_phase_history`` returns a registered fak
 (``pfa_b200.synth.FakeReader``) for a synthetic scene.  Nothing in the reference is patched.
 
 Used by ``tests/golden/make_golden.py`` and by CPU tests that pin the oracle against the reference.
-It only works where the reference checkout exists (``PFA_REFERENCE_ROOT``, default
-``/root/reference``); the GPU tests, ``smoke()`` and ``bench.py`` never import it.
+It only works where the reference checkout exists (``PFA_REFERENCE_ROOT``, default: a ``reference``
+checkout beside this repository); the GPU tests, ``smoke()`` and ``bench.py`` never import it.
 """
 from __future__ import annotations
 
@@ -19,7 +19,7 @@ import sys
 import types
 from pathlib import Path
 
-REF_ROOT = Path(os.environ.get("PFA_REFERENCE_ROOT", "/root/reference"))
+REF_ROOT = Path(os.environ.get("PFA_REFERENCE_ROOT", Path(__file__).resolve().parents[2] / "reference"))
 _READERS: dict[str, object] = {}
 
 

@@ -1,6 +1,6 @@
 """Generate the golden fixtures in this folder by running the UNMODIFIED reference.
 
-Run where the reference checkout exists (default /root/reference, or PFA_REFERENCE_ROOT):
+Run where the reference checkout exists (a ``reference`` checkout beside this repository, or PFA_REFERENCE_ROOT):
 
     python tests/golden/make_golden.py            # small fixed/float cases + FFT KAT digests
     python tests/golden/make_golden.py --big      # also the 5634x4319 -> 8192^2 sinc/sinc frame

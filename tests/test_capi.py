@@ -32,8 +32,9 @@ def test_library_exports_every_declared_symbol():
 def test_status_strings_and_version():
     lib = _lib.load()
     assert lib.pfa_version().startswith(b"pfa_b200")
-    for st in range(9):
-        assert lib.pfa_status_string(st)
+    strings = [lib.pfa_status_string(st) for st in range(10)]
+    assert all(strings) and len(set(strings)) == 10
+    assert b"1024" in strings[_lib.TOO_LARGE]
     assert lib.pfa_status_string(99) == b"unknown status"
 
 
@@ -86,3 +87,29 @@ def test_fixed_job_matches_oracle_geometry():
     assert np.array_equal(job["order"], geo["order"])
     with pytest.raises(ValueError):
         geometry.fixed_job(tb, 256)
+
+
+def test_noalloc_validates_before_touching_a_device():
+    """The allocation-free entry point refuses a non-permutation inv_order (PFA_ERR_BAD_ARG), a grid above
+    its static scratch (PFA_ERR_TOO_LARGE) and dims above the grid (PFA_ERR_BAD_DIMS) on the host, before
+    any device call; the signal and image pointers are never dereferenced on these paths."""
+    from pfa_b200 import synth
+    lib = _lib.load()
+    sc = synth.make_scene(120, 100, n_targets=2, seed=5, with_signal=False)
+    tb = geometry.prepare_tables_from_scene(sc)
+    j = geometry.fixed_job(tb, 256)
+    inv = np.empty(j["m"], np.int32)
+    inv[j["order"]] = np.arange(j["m"], dtype=np.int32)
+    inv[1] = inv[0]                               # duplicate slot: not a permutation
+    keep = [j["f0"], j["df"], j["pr"], j["tan_s"], inv, j["krp"], j["kcp"],
+            np.ascontiguousarray(j["hamr"], np.int32), np.ascontiguousarray(j["hamc"], np.int32),
+            np.ascontiguousarray(j["twiddle"], np.int16)]
+    job = _lib.FixedJob(*[ctypes.c_void_p(a.ctypes.data) for a in keep], None)
+    fake_sig, fake_img = ctypes.c_void_p(1 << 20), ctypes.c_void_p(2 << 20)    # aligned, never read
+    cfg = _lib.Config(mode=_lib.MODE_FIXED, m=120, n=100, grid=256, range_interp=_lib.SINC, az_interp=_lib.SINC)
+    assert lib.pfa_form_fixed_noalloc(ctypes.byref(cfg), ctypes.byref(job), fake_sig, fake_img, None) == _lib.BAD_ARG
+    cfg.grid = 2048
+    assert lib.pfa_form_fixed_noalloc(ctypes.byref(cfg), ctypes.byref(job), fake_sig, fake_img, None) == _lib.TOO_LARGE
+    cfg.grid, cfg.m = 64, 120
+    assert lib.pfa_form_fixed_noalloc(ctypes.byref(cfg), ctypes.byref(job), fake_sig, fake_img, None) == _lib.BAD_DIMS
+    assert lib.pfa_form_fixed_noalloc(ctypes.byref(cfg), ctypes.byref(job), None, fake_img, None) == _lib.BAD_ARG

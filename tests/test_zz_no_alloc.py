@@ -4,8 +4,10 @@ It exists for callers that cannot allocate device memory (a host that owns all d
 its own pool, a real-time loop that must not touch the allocator, a process whose allocator is
 exhausted).  It keeps its scratch in one static device array, so this test calls it through the C ABI
 twice in a row on different frames (the second call must not see the first call's leftovers) and checks
-each image against the planned entry point pfa_form_fixed, bit for bit (the fixed-point tolerance is 0).
-It also checks that a frame above the array's limit (grid 1024) is rejected with PFA_ERR_TOO_LARGE.
+each image against the planned entry point pfa_form_fixed and against the CPU oracle of the emulator's
+datapath, bit for bit (the fixed-point tolerance is 0).  One of the calls passes its own copy of the sinc
+table (the caller-supplied table branch).  It also checks that a frame above the array's limit (grid 1024)
+is rejected with PFA_ERR_TOO_LARGE.
 This file is collected last so that a run stopping at the first failure has run every other test.
 """
 import ctypes as C
@@ -13,27 +15,30 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from oracle import fixed_emulator as fe
 from pfa_b200 import _lib, engine, geometry, synth
 
 pytestmark = pytest.mark.gpu
 
 
-def _job(tables, grid):
+def _job(tables, grid, sinc=None):
     j = geometry.fixed_job(tables, grid)
     inv = np.empty(j["m"], np.int32)
     inv[j["order"]] = np.arange(j["m"], dtype=np.int32)
     keep = [j["f0"], j["df"], j["pr"], j["tan_s"], inv, j["krp"], j["kcp"],
             np.ascontiguousarray(j["hamr"], np.int32), np.ascontiguousarray(j["hamc"], np.int32),
             np.ascontiguousarray(j["twiddle"], np.int16)]
-    ptrs = [C.c_void_p(a.ctypes.data) for a in keep] + [None]
+    if sinc is not None:
+        keep.append(np.ascontiguousarray(sinc, np.int16))
+    ptrs = [C.c_void_p(a.ctypes.data) for a in keep] + ([] if sinc is not None else [None])
     return _lib.FixedJob(*ptrs), keep
 
 
-def _noalloc(torch, sig, tables, grid, rs, az):
+def _noalloc(torch, sig, tables, grid, rs, az, sinc=None):
     lib = _lib.load()
     m, n = sig.shape
     cfg = _lib.Config(mode=_lib.MODE_FIXED, m=m, n=n, grid=grid, range_interp=int(rs), az_interp=int(az), device=0)
-    job, keep = _job(tables, grid)
+    job, keep = _job(tables, grid, sinc)
     x = torch.from_numpy(np.ascontiguousarray(sig)).cuda()
     img = torch.empty((grid, grid), dtype=torch.uint16, device="cuda")
     st = lib.pfa_form_fixed_noalloc(C.byref(cfg), C.byref(job), C.c_void_p(x.data_ptr()), C.c_void_p(img.data_ptr()),
@@ -54,16 +59,21 @@ def test_noalloc_matches_planned_entry_point_on_two_calls():
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
+    # the reference's own table, passed explicitly in the second call ([phase][tap] int16, host memory)
+    own_sinc = np.array(fe._tab(), dtype=np.int16).reshape(256, 32)
     cases = [
-        (synth.make_scene(900, 1000, n_targets=16, clutter_db=-10.0, snr_db=20.0, seed=41, jitter=0.3), 1024, True, True),
-        (synth.make_scene(300, 250, n_targets=8, snr_db=20.0, seed=42), 512, False, True),
+        (synth.make_scene(900, 1000, n_targets=16, clutter_db=-10.0, snr_db=20.0, seed=41, jitter=0.3), 1024, True, True,
+         None),
+        (synth.make_scene(300, 250, n_targets=8, snr_db=20.0, seed=42), 512, False, True, own_sinc),
     ]
-    for sc, grid, rs, az in cases:
+    for sc, grid, rs, az, sinc in cases:
         tables = geometry.prepare_tables_from_scene(sc)
-        got = _noalloc(torch, sc.signal, tables, grid, rs, az)
+        got = _noalloc(torch, sc.signal, tables, grid, rs, az, sinc)
         want = _planned(torch, sc.signal, tables, grid, rs, az)
         assert got.shape == want.shape
         assert np.array_equal(got, want), f"{(got != want).sum()} pixels differ"
+        ref, _ = fe.form_image(sc.signal, tables, grid, range_sinc=rs, az_sinc=az)
+        assert np.array_equal(got, ref), f"{(got != ref).sum()} pixels differ from the oracle"
         assert got.any()
 
 
