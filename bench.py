@@ -13,9 +13,10 @@ copies inside the timed region; uploads and downloads overlap neighbouring frame
 collective on the data path).  Inputs (195 MB signal, 268 MB FFT-2 buffer) exceed the 126 MB L2, so
 no explicit flush is done between frames.
 
---impl reference times the CPU restatement of the reference's emulator (the oracle port; the
-reference itself is Python and does not travel) on a bounded sample of the frame's lines per step,
-using every host core, and prints the same JSON line with "impl": "reference".
+--impl reference times the CPU restatement of the reference's emulator (the oracle port in C; the
+reference itself is Python and does not travel): one whole frame per step on every host core, its
+image CRC checked against the reference emulator's; it prints the same JSON line with
+"impl": "reference".
 """
 from __future__ import annotations
 
@@ -41,7 +42,9 @@ WORKLOADS = {
     "centerfield_5634x4319": dict(mode="fixed", grid=8192, range_sinc=True, az_sinc=True, scene="centerfield_5634x4319",
                                   desc="Centerfield-shaped 5634x4319 c64 -> 8192^2, fixed point, "
                                        "--deci 1 --grid 8192 --range-sinc --az-sinc, 256 targets + "
-                                       "Rayleigh clutter -10 dB, seed 2"),
+                                       "Rayleigh clutter -10 dB, seed 2",
+                                  # CRC-32 of the unmodified reference emulator's image of this frame
+                                  ref_crc=0x7A44896A, ref_emulator_s=176.7),
     "ndsu_8167x8192_fp32": dict(mode="float", mixed=False, range_sinc=False, az_sinc=False, scene="ndsu_8167x8192",
                                 desc="NDSU-shaped 8167x8192 c64 -> 8192^2, float FP32 (lerp, form_image_pfa), "
                                      "1024 targets + Rayleigh clutter -10 dB, 15 dB SNR, seed 3"),
@@ -185,11 +188,58 @@ def cpu_float_small(sc, tables):
             "sample": "whole 1024x1024 frame, form_image_pfa restated (lerp), best of 3"}
 
 
+def _float_e2e(sig, tables, local):
+    """FP32 lerp frames end to end through the pipelined host-buffer entry point (pinned host in/out)."""
+    import torch
+    from pfa_b200 import engine
+    sig_h = torch.empty(tuple(sig.shape), dtype=torch.complex64).pin_memory()
+    sig_h.copy_(sig)
+    outs_h = [torch.empty((8192, 8192), dtype=torch.float32).pin_memory() for _ in range(2)]
+    with engine.FloatPlan(8167, 8192, device=local) as hp:
+        hp.set_tables(tables)
+        frames = [sig_h.numpy()] * 4
+        outs = [outs_h[k & 1].numpy() for k in range(4)]
+        hp.form_host_frames(frames[:2], outs[:2])
+        t0 = time.perf_counter()
+        hp.form_host_frames(frames, outs)
+        ms = round((time.perf_counter() - t0) * 1000.0 / 4, 4)
+    return ms, {"h2d": int(sig_h.numel() * 8), "d2h": 8192 * 8192 * 4}
+
+
+def float_cpu_leg(sig_np, tables, interp, imgs):
+    """CPU baseline and FP64 checker of the production-shape float frame (8167x8192 -> 8192^2).
+
+    lerp: the reference-precision restatement of form_image_pfa.resample_kspace + focus + |.| (complex64,
+    np.interp, NumPy FFT) over the whole frame on one core is the cpu_baseline; the FP64 restatement of the
+    same algorithm is the checker.  sinc: the reference has no float sinc, so the FP64 restatement of the
+    float sinc (over all host cores) is both.  Returns (cpu_baseline dict, {mixed: errors vs FP64})."""
+    from oracle import cpu_sample, float_pfa as fp
+    cores = cpu_sample.available_cores()
+    t0 = time.perf_counter()
+    r64 = fp.pfa_image(sig_np, tables["freq"], tables["ax"], tables["ay"], tables["sgn"], precision="f64",
+                       interp=interp, threads=cores if interp == "sinc" else 1)
+    t64 = time.perf_counter() - t0
+    if interp == "lerp":
+        t0 = time.perf_counter()
+        fp.detect(fp.pfa_image(sig_np, tables["freq"], tables["ax"], tables["ay"], tables["sgn"], precision="ref"))
+        cpu = {"value": round((time.perf_counter() - t0) * 1000.0, 1), "unit": "ms/frame", "cores": 1, "kind": "port",
+               "sample": "whole 8167x8192 frame, form_image_pfa restated at its own precision (np.interp passes, "
+                         "complex64, NumPy FFT, |z|)"}
+    else:
+        cpu = {"value": round(t64 * 1000.0, 1), "unit": "ms/frame", "cores": cores, "kind": "port",
+               "sample": "whole 8167x8192 frame, FP64 restatement of the float 32-tap sinc PFA (the reference "
+                         "has no float sinc), sinc lines over a thread pool"}
+    errs = {mixed: fp.error_report(img, r64, k=64) for mixed, img in imgs.items()}
+    return cpu, errs
+
+
 def measure_modes(a, local):
     """The other configurations of the metric, device-timed at N=1: the NDSU-shaped float frame
     (8167x8192 -> 8192^2; FP32 lerp as form_image_pfa, FP32 32-tap sinc, and both in the split-precision
-    tensor-core FFT mode with its error against the FP32 image), the image-entropy autofocus gradient on
-    the 4096^2 scene (grads/s) and the 16-scene batch."""
+    tensor-core FFT mode), each with its errors against the FP64 oracle image (relative L2 of the complex
+    and detected image, phase RMS, peak position / power and ISLR of the 64 strongest point responses)
+    and a CPU baseline, the image-entropy autofocus gradient on the 4096^2 scene (grads/s) and the
+    16-scene batch."""
     import numpy as np
     import torch
     from pfa_b200 import autofocus, engine, geometry, synth
@@ -212,46 +262,43 @@ def measure_modes(a, local):
     del sig1
     sc, sig = synth.make_scene_device(8167, 8192, device=f"cuda:{local}", **{k: v for k, v in synth.WORKLOADS["ndsu_8167x8192"].items() if k not in ("m", "n")})
     tables = geometry.prepare_tables_from_scene(sc)
-    ref_c = {}
-    for name, rs, mixed in (("float_fp32_lerp", False, False), ("float_fp32_sinc", True, False),
-                            ("float_mixed_lerp", False, True), ("float_mixed_sinc", True, True)):
-        with engine.FloatPlan(8167, 8192, rs, rs, mixed=mixed, device=local) as plan:
-            plan.set_tables(tables)
-            img = torch.empty((8192, 8192), dtype=torch.float32, device=sig.device)
-            ms = _device_ms(lambda: plan.form(sig, out=img), steps, 3)
-            plan.set_profiling(True)
-            plan.form(sig, out=img)
-            st = plan.stage_times()
-            plan.set_profiling(False)
-            cz = plan.form(sig, detect="complex")
-        fb = sum(stage_bytes(s, 8167, 8192, 8192, "float") for s in st)
-        out[name] = {"workload": "ndsu_8167x8192 -> 8192^2", "ms_per_frame": round(ms, 4),
-                     "stages_ms": {k: round(v, 4) for k, v in st.items()},
-                     "frame_bytes": fb, "frame_frac_of_hbm": round(fb / (ms * 1e-3) / 1e9 / _peaks()[0], 4)}
-        if name == "float_fp32_lerp":
-            # end to end through the pipelined host-buffer entry point (pinned host in/out, PCIe included)
-            sig_h = torch.empty(tuple(sig.shape), dtype=torch.complex64).pin_memory()
-            sig_h.copy_(sig)
-            outs_h = [torch.empty((8192, 8192), dtype=torch.float32).pin_memory() for _ in range(2)]
-            with engine.FloatPlan(8167, 8192, device=local) as hp:
-                hp.set_tables(tables)
-                frames = [sig_h.numpy()] * 4
-                outs = [outs_h[k & 1].numpy() for k in range(4)]
-                hp.form_host_frames(frames[:2], outs[:2])
-                t0 = time.perf_counter()
-                hp.form_host_frames(frames, outs)
-                out[name]["e2e_ms_per_frame"] = round((time.perf_counter() - t0) * 1000.0 / 4, 4)
-                out[name]["e2e_bytes_per_frame"] = {"h2d": int(sig_h.numel() * 8), "d2h": 8192 * 8192 * 4}
-            del sig_h, outs_h
-        if not mixed:
-            ref_c[rs] = (cz, ms)
-        else:
-            # the FP32 image is pinned to FP64 at <= 1e-6 (tests); the mixed error budget is 1e-4
-            r, ms32 = ref_c[rs]
-            out[name]["rel_l2_vs_fp32_complex"] = float(torch.linalg.vector_norm(cz - r) / torch.linalg.vector_norm(r))
-            out[name]["speed_vs_fp32"] = round(ms32 / ms, 3)
-        del cz
-    ref_c.clear()
+    sig_np = sig.cpu().numpy() if not a.no_cpu_baseline else None
+    for interp, rs in (("lerp", False), ("sinc", True)):
+        imgs = {}
+        for mixed in (False, True):
+            name = f"float_{'mixed' if mixed else 'fp32'}_{interp}"
+            with engine.FloatPlan(8167, 8192, rs, rs, mixed=mixed, device=local) as plan:
+                plan.set_tables(tables)
+                img = torch.empty((8192, 8192), dtype=torch.float32, device=sig.device)
+                ms = _device_ms(lambda: plan.form(sig, out=img), steps, 3)
+                plan.set_profiling(True)
+                plan.form(sig, out=img)
+                st = plan.stage_times()
+                plan.set_profiling(False)
+                cz = plan.form(sig, detect="complex")
+            fb = sum(stage_bytes(s_, 8167, 8192, 8192, "float") for s_ in st)
+            out[name] = {"workload": "ndsu_8167x8192 -> 8192^2", "ms_per_frame": round(ms, 4),
+                         "stages_ms": {k: round(v, 4) for k, v in st.items()},
+                         "frame_bytes": fb, "frame_frac_of_hbm": round(fb / (ms * 1e-3) / 1e9 / _peaks()[0], 4)}
+            if name == "float_fp32_lerp":
+                out[name]["e2e_ms_per_frame"], out[name]["e2e_bytes_per_frame"] = _float_e2e(sig, tables, local)
+            if mixed:
+                r, ms32 = imgs[False]
+                out[name]["rel_l2_vs_fp32_complex"] = float(torch.linalg.vector_norm(cz - r) / torch.linalg.vector_norm(r))
+                out[name]["speed_vs_fp32"] = round(ms32 / ms, 3)
+            imgs[mixed] = (cz, ms)
+        if not a.no_cpu_baseline:
+            # the cpu_baseline leg: the oracle's restatement of form_image_pfa over the whole frame on the
+            # host, timed; its FP64 image is also the checker of both device images' errors
+            host = {k: v[0].cpu().numpy() for k, v in imgs.items()}
+            imgs.clear()
+            cpu, errs = float_cpu_leg(sig_np, tables, interp, host)
+            for mixed, e in errs.items():
+                nm = f"float_{'mixed' if mixed else 'fp32'}_{interp}"
+                out[nm]["vs_fp64"] = e
+                out[nm]["cpu_baseline"] = cpu
+            del host
+        imgs.clear()
     del sig
     wl = synth.WORKLOADS["autofocus_4096"]
     sc, sig = synth.make_scene_device(4096, 4096, device=f"cuda:{local}", **{k: v for k, v in wl.items() if k not in ("m", "n")})
@@ -268,12 +315,23 @@ def measure_modes(a, local):
         autofocus.entropy_grad(plan, sig, theta, dth, ent)
         st = plan.stage_times()
         plan.set_profiling(False)
-        _, hist = autofocus.autofocus(plan, sig, steps=50, step=0.3, history=True)
+        th50, hist = autofocus.autofocus(plan, sig, steps=50, step=0.3, history=True)
+        # focus quality: the entropy of the image with the injected error removed exactly (theta = phi)
+        # and the residual phase error after 50 steps, without the constant and linear terms (a constant
+        # phase leaves the image unchanged, a linear one only shifts it)
+        e_true, _ = autofocus.entropy_grad(plan, sig, phi.float())
+        res = (th50.double() - phi).cpu().numpy()
+        u = np.arange(4096, dtype=np.float64)
+        res = res - np.polyval(np.polyfit(u, res, 1), u)
+        res0 = phi.cpu().numpy() - np.polyval(np.polyfit(u, phi.cpu().numpy(), 1), u)
     out["autofocus_4096"] = {"workload": "4096x4096 c64, 128 targets + clutter, quadratic 3 rad + random walk "
                                          "0.05 rad/pulse phase error; entropy gradient w.r.t. 4096 phases",
                              "ms_per_grad": round(ms, 4), "grads_per_s": round(1000.0 / ms, 1),
                              "stages_ms": {k: round(v, 4) for k, v in st.items()},
-                             "entropy_first_last_of_50_steps": [round(hist[0], 5), round(hist[-1], 5)]}
+                             "entropy_first_last_of_50_steps": [round(hist[0], 5), round(hist[-1], 5)],
+                             "entropy_true_phase": round(float(e_true), 5),
+                             "phase_rms_rad_before_after_50_steps": [round(float(np.sqrt(np.mean(res0 ** 2))), 4),
+                                                                     round(float(np.sqrt(np.mean(res ** 2))), 4)]}
     del sig
     out["batch_16_uneven"] = measure_batch(a, local)
     return out
@@ -424,12 +482,17 @@ def run_ours(a, ws, rank, local):
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         from oracle import cpu_sample
         if mode == "fixed":
-            est = cpu_sample.fixed_frame_estimate(sc.signal, tables, G, wl["range_sinc"], wl["az_sinc"],
-                                                  sample=a.cpu_sample, workers=1)
+            # the C restatement of the emulator's datapath, one whole frame on one core
+            t0 = time.perf_counter()
+            ref_img, _ = cpu_sample.c_fixed_frame(sc.signal, tables, G, wl["range_sinc"], wl["az_sinc"], threads=1)
+            cpu = {"value": round((time.perf_counter() - t0) * 1000.0, 1), "unit": "ms/frame", "cores": 1,
+                   "kind": "port", "sample": "one whole frame of the C restatement of the emulator datapath "
+                                             "(oracle/fixed_frame.c), 1 thread",
+                   "image_equal_to_gpu": bool(np.array_equal(ref_img, img.cpu().numpy()))}
         else:
             est = cpu_sample.float_frame_estimate(sc.signal, tables, sample=a.cpu_sample, workers=1)
-        cpu = {"value": round(est["ms_per_frame"], 1), "unit": "ms/frame", "cores": 1, "kind": "port",
-               "sample": est["sample"], "stage_seconds": est["stage_seconds"]}
+            cpu = {"value": round(est["ms_per_frame"], 1), "unit": "ms/frame", "cores": 1, "kind": "port",
+                   "sample": est["sample"], "stage_seconds": est["stage_seconds"]}
 
     line = {
         "metric": METRIC, "value": round(ms_per_frame, 4), "unit": "ms/frame", "n_gpus": ws,
@@ -472,10 +535,18 @@ def run_ours(a, ws, rank, local):
 
 
 def run_reference(a, ws, rank):
+    """The reference arm: the CPU restatement of the reference's path on every host core, rank 0 only.
+
+    Fixed workload: every step (warm-up and timed) forms one WHOLE frame with the C restatement of the
+    emulator's datapath (oracle/fixed_frame.c, OpenMP over all host threads); the first frame's CRC is
+    checked against the unmodified reference emulator's CRC of the same frame.  Float workloads: the
+    sampled estimate of form_image_pfa's restatement (spawned workers)."""
     if rank != 0:
         return
+    import numpy as np
     from pfa_b200 import geometry, synth
     from oracle import cpu_sample
+    from oracle import fixed_emulator as fe
     wl = WORKLOADS[a.workload]
     sc = synth.workload_scene(wl["scene"])
     m, n = sc.signal.shape
@@ -483,32 +554,48 @@ def run_reference(a, ws, rank):
     tables = geometry.prepare_tables_from_scene(sc)
     cores = cpu_sample.available_cores()
     per = []
-    pool = cpu_sample.make_pool(cores) if cores > 1 else None
-    try:
+    extra = {}
+    if wl["mode"] == "fixed":
         for i in range(a.warmup + a.steps):
-            if wl["mode"] == "fixed":
-                est = cpu_sample.fixed_frame_estimate(sc.signal, tables, G, wl["range_sinc"], wl["az_sinc"],
-                                                      sample=a.ref_sample, workers=cores, seed=i, pool=pool)
-            else:
+            t0 = time.perf_counter()
+            img, _ = cpu_sample.c_fixed_frame(sc.signal, tables, G, wl["range_sinc"], wl["az_sinc"], threads=cores)
+            dt = (time.perf_counter() - t0) * 1000.0
+            if i == 0 and "ref_crc" in wl:
+                crc = fe.frame_crc(img)
+                extra["image_crc"] = f"0x{crc:08x}"
+                extra["crc_equals_reference_emulator"] = crc == wl["ref_crc"]
+            if i >= a.warmup:
+                per.append(dt)
+        sample = (f"whole frame per step: C restatement of the emulator datapath (oracle/fixed_frame.c), "
+                  f"OpenMP, {cores} threads")
+        dtype = "int16 fixed point (int32/int64 C)"
+        if "ref_emulator_s" in wl:
+            extra["context"] = {"reference_emulator_whole_frame_ms_1_core": wl["ref_emulator_s"] * 1000.0,
+                                "note": "the unmodified NumPy emulator, measured once on this frame"}
+    else:
+        pool = cpu_sample.make_pool(cores) if cores > 1 else None
+        try:
+            for i in range(a.warmup + a.steps):
                 est = cpu_sample.float_frame_estimate(sc.signal, tables, sample=a.ref_sample, workers=cores,
                                                       seed=i, pool=pool)
-            if i >= a.warmup:
-                per.append(est["ms_per_frame"])
-    finally:
-        if pool is not None:
-            pool.shutdown()
+                if i >= a.warmup:
+                    per.append(est["ms_per_frame"])
+        finally:
+            if pool is not None:
+                pool.shutdown()
+        sample = est["sample"] + f"; {cores} spawned worker processes"
+        dtype = "complex64/float64 numpy"
     v = statistics.mean(per)
     line = {
         "metric": METRIC, "value": round(v, 1), "unit": "ms/frame", "n_gpus": ws, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(v, 1), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": round(v / FPGA_FRAME_MS[a.workload], 6) if a.workload in FPGA_FRAME_MS else None,
-        "dtype": "int16 fixed point (int64 numpy)" if wl["mode"] == "fixed" else "complex64/float64 numpy",
-        "data": "synthetic", "impl": "reference",
+        "dtype": dtype, "data": "synthetic", "impl": "reference",
         "config": {"workload": a.workload, "desc": wl["desc"], "m": m, "n": n, "grid": G},
-        "cpu_baseline": {"value": round(v, 1), "unit": "ms/frame", "cores": cores, "kind": "port",
-                         "sample": est["sample"] + f"; {cores} spawned worker processes"},
+        "cpu_baseline": {"value": round(v, 1), "unit": "ms/frame", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": round(v, 1), "unit": "ms/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    line.update(extra)
     print(json.dumps(line), flush=True)
 
 

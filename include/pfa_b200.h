@@ -203,6 +203,19 @@ pfa_status pfa_form_float_host(pfa_plan *plan, const float *sig_host, void *out_
 pfa_status pfa_autofocus_grad(pfa_plan *plan, const float *sig_dev, const float *theta_dev, float *dtheta_dev,
                               double *entropy_dev, void *stream);
 
+/* Display scaling of the detected float image, the quantiser of save_detected_geotiff
+ * (src/form_image_pfa.py:287-292): hi = np.percentile(amp, percentile) and
+ * out = uint8(clip(amp / (hi + 1e-12) * 255, 0, 255)), bit-exact to NumPy's float32 arithmetic, for
+ * non-negative magnitudes amp (PFA_DETECT_MAG output).  mag_dev: float32 [count], 16-byte aligned;
+ * out_dev: uint8 [count], 4-byte aligned; hi_dev (float32, device) may be NULL.  workspace_dev: at least
+ * pfa_display_workspace_bytes() device bytes, 8-byte aligned, owned by the caller (no allocation, no host
+ * synchronisation; calls sharing a workspace must not overlap).  The percentile is found by a radix select
+ * over the float bit patterns on the device (three histogram passes plus one for the next order statistic).
+ * The reference writes these bytes to its GeoTIFF; pfa_b200.geocode adds the map affine and the file. */
+size_t pfa_display_workspace_bytes(void);
+pfa_status pfa_display_u8(const float *mag_dev, int64_t count, float percentile, void *workspace_dev, uint8_t *out_dev,
+                          float *hi_dev, void *stream);
+
 /* Per-stage device timing, the counterpart of the board's per-stage timestamps sar_stage_ts[]
  * (sar_sequencer.c:235-238) and form_image_pfa.StepTimer (src/form_image_pfa.py:42-60).  When enabled,
  * every form call records CUDA events between its kernels on the launching stream.

@@ -19,7 +19,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]
-SOURCES = ["pfa_capi.cu", "pfa_fixed.cu", "pfa_float.cu", "pfa_mixed.cu", "pfa_noalloc.cu"]
+SOURCES = ["pfa_capi.cu", "pfa_fixed.cu", "pfa_float.cu", "pfa_mixed.cu", "pfa_noalloc.cu", "pfa_display.cu"]
 
 
 def _gen():

@@ -232,11 +232,15 @@ __global__ void __launch_bounds__(256, SINC ? 3 : 4) k_fl_pass1(FPass1Args a) {
     }
 }
 
-// packed pass-2 bracket (written by the lerp pass 2 for the autofocus adjoint): bit 31 = outside the span, bits 17..30 = lower index, bits 0..16 = weight
+// packed pass-2 bracket (written by the forward pass 2 of an autofocus gradient for the adjoint), on the
+// ascending view of the pass-2 sources: bit 31 = outside the span, bits 17..30 = lower index ja, bits 0..16 =
+// the lerp weight toward ja + 1 (x 131071) or, for an interior bracket of the float sinc (15 <= ja <= m-17,
+// where no lerp weight is needed), the sinc phase
 __device__ __forceinline__ uint32_t pack_br(int dead, int lowi, float f) {
     const uint32_t q = (uint32_t)fminf(fmaxf(rintf(f * 131071.f), 0.f), 131071.f);
     return ((uint32_t)dead << 31) | ((uint32_t)lowi << 17) | q;
 }
+__device__ __forceinline__ uint32_t pack_br_phase(int lowi, int ph) { return ((uint32_t)lowi << 17) | (uint32_t)ph; }
 __device__ __forceinline__ int br_low(uint32_t p) { return (int)((p >> 17) & 0x3fffu); }
 
 // ------------------------------------------------------------------------------------------ K2f
@@ -313,6 +317,16 @@ k_fl_pass2_fft(FPass2Args a) {
 #pragma unroll
         for (int c = 0; c < CH; ++c) {
             const int u = u0 + c;
+            if constexpr (PK) {
+                // the adjoint's brackets on the ascending view (fraction and phase before any mirroring)
+                if (ok[c]) {
+                    uint32_t pkv;
+                    if (ja[c] < 0) pkv = pack_br(1, q[c] < lo_v ? 0 : m - 2, 0.f);
+                    else if (SINC && ja[c] >= 15 && ja[c] <= m - 17) pkv = pack_br_phase(ja[c], fr[c].ph);
+                    else pkv = pack_br(0, ja[c], fr[c].f);
+                    a.pk_out[(size_t)j * m + tid + T * u] = pkv;
+                }
+            }
             bl[u] = -1;
             bf[u] = 0.f;
             if (ja[c] >= 0) {
@@ -320,12 +334,6 @@ k_fl_pass2_fft(FPass2Args a) {
                 if (!asc) { lowi = m - 2 - ja[c]; mirror_frac(fr[c]); }
                 bl[u] = lowi | (fr[c].ph << 16) | (fr[c].rev << 24);
                 bf[u] = fr[c].f;
-            }
-            if constexpr (PK && !SINC) {
-                // the adjoint's brackets (ascending sources: the autofocus plan has KR > 0)
-                if (ok[c])
-                    a.pk_out[(size_t)j * m + tid + T * u] =
-                        ja[c] >= 0 ? pack_br(0, ja[c], fr[c].f) : pack_br(1, q[c] < lo_v ? 0 : m - 2, 0.f);
             }
         }
     }
@@ -522,8 +530,10 @@ k_af_range_adjoint(AfRangeArgs a) {
 struct AfCrossArgs {
     const float2 *zadj_t;   // [n][m2]
     const float2 *p1;       // [n][mpad] forward pass-1 output (phase corrected)
-    const uint32_t *pk;     // [n][m] packed brackets of the forward pass 2
+    const uint32_t *pk;     // [n][m] packed brackets of the forward pass 2 (ascending view)
     const double *ham_m, *ham_n;
+    const double *kr_grid, *tan_s;   // the direction of range bin j's pass-2 source axis
+    const int16_t *tabq;    // float sinc table (Q15 taps, [phase][kTabRow])
     const float2 *tw;       // cross twiddles (m2)
     float *dacc;            // [mpad] per-slot Im sum conj(g_p1) p1
     int m, n, mpad, window;
@@ -537,21 +547,35 @@ __device__ __forceinline__ int pk_at(int k) { return k ^ ((k >> 5) & 15); }
 __device__ __forceinline__ int y_at(int k) { return k ^ ((k >> 4) & 15); }
 __device__ __forceinline__ float br_w(uint32_t p) { return (float)(p & 0x1ffffu) * (1.0f / 131071.f); }
 
-template <int L, int E>
+// R2^H as an atomics-free segmented reduction.  On the ascending view of the sources, bracket k (lower index
+// l_k, monotone in k) touches slots l_k and l_k + 1 (lerp: weights 1 - f and f) or, for an interior float
+// sinc bracket, slots l_k - 15 .. l_k + 16 (weight tab[phase][u - l_k + 15] / 2^15).  So slot u collects
+// the contiguous run of k with l_k in [u - 16, u + 15] (sinc) or [u - 1, u] (lerp), and each thread walks
+// one run for its E consecutive slots.  A descending source axis maps ascending slot u to natural slot
+// m - 1 - u (the forward mirrors the bracket and reverses the taps, which is the same linear map).
+template <int L, int E, bool SINC>
 __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_adjoint(AfCrossArgs a) {
     using F = F32Fft<L, E>;
     constexpr int N = F::N, T = F::T;
+    constexpr int REACH_LO = SINC ? 16 : 1, REACH_HI = SINC ? 15 : 0;
     extern __shared__ __align__(16) unsigned char smem[];
     float2 *xbuf = reinterpret_cast<float2 *>(smem);
     uint32_t *pk = reinterpret_cast<uint32_t *>(smem + (size_t)8 * F::xbuf_elems());
     const int tid = threadIdx.x;
     const int j = blockIdx.x;                         // range bin (< n)
     const int m = a.m;
+    int16_t *tab = reinterpret_cast<int16_t *>(smem + (size_t)8 * F::xbuf_elems() + (size_t)4 * ((m + 15) & ~15));
     // the forward pass-2 brackets of this range bin (stored by the forward pass 2 of this gradient)
     {
         const uint32_t *src = a.pk + (size_t)j * m;
         for (int k = tid; k < m; k += T) pk[pk_at(k)] = __ldcs(src + k);
+        if (SINC) {
+            const uint4 *t4 = reinterpret_cast<const uint4 *>(a.tabq);
+            for (int c = tid; c < kTabShorts / 8; c += T) reinterpret_cast<uint4 *>(tab)[c] = __ldg(t4 + c);
+        }
     }
+    const double krj = a.kr_grid[j];
+    const bool asc = krj * a.tan_s[m - 1] >= krj * a.tan_s[0];    // as the forward pass 2 decides
     // adjoint of the cross FFT
     const float2 *row = a.zadj_t + (size_t)j * N;
     float2 x[E];
@@ -571,17 +595,15 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
         xbuf[y_at(k)] = make_float2(w * x[v].x, -w * x[v].y);   // W . F_cross^H g, cross index k
     }
     __syncthreads();
-    // R2^H, atomics free: slot r collects bracket k with lower index r (weight 1-f) and r-1 (weight f);
-    // the lower index is monotone in k, so each thread walks one contiguous run of k for its E slots
     const int r_lo = tid * E;
     float2 gs[E];
 #pragma unroll
     for (int s2 = 0; s2 < E; ++s2) gs[s2] = make_float2(0.f, 0.f);
     if (r_lo < m) {
-        int lo = 0, hi = m;                             // first k with lower index >= r_lo - 1
+        int lo = 0, hi = m;                             // first k with lower index >= r_lo - REACH_LO
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
-            if (br_low(pk[pk_at(mid)]) < r_lo - 1) lo = mid + 1; else hi = mid;
+            if (br_low(pk[pk_at(mid)]) < r_lo - REACH_LO) lo = mid + 1; else hi = mid;
         }
         int kp = lo;
 #pragma unroll
@@ -592,15 +614,21 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
                 for (int kk = kp; kk < m; ++kk) {
                     const uint32_t b = pk[pk_at(kk)];
                     const int l = br_low(b);
-                    if (l > r) break;
+                    if (l > r + REACH_HI) break;
                     if (b >> 31) continue;
-                    const float f = br_w(b);
-                    const float wgt = (l == r) ? 1.0f - f : (l == r - 1 ? f : 0.f);
+                    float wgt;
+                    if (SINC && l >= 15 && l <= m - 17) {
+                        const int t = r - l + 15;
+                        wgt = (t >= 0 && t < 32) ? (float)tab[(b & 0xffu) * kTabRow + t] * (1.0f / 32768.f) : 0.f;
+                    } else {
+                        const float f = br_w(b);
+                        wgt = (l == r) ? 1.0f - f : (l == r - 1 ? f : 0.f);
+                    }
                     const float2 y = xbuf[y_at(kk)];
                     gsum.x = fmaf(wgt, y.x, gsum.x);
                     gsum.y = fmaf(wgt, y.y, gsum.y);
                 }
-                while (kp < m && br_low(pk[pk_at(kp)]) < r) ++kp;
+                while (kp < m && br_low(pk[pk_at(kp)]) < r + 1 - REACH_LO) ++kp;
                 gs[s2] = gsum;
             }
         }
@@ -620,9 +648,9 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
     }
 #pragma unroll
     for (int v = 0; v < E; ++v) {
-        const int r = tid + T * v;
+        const int r = tid + T * v;                    // natural slot
         if (r < m) {
-            const float2 g = xbuf[F::pad(r)];
+            const float2 g = xbuf[F::pad(asc ? r : m - 1 - r)];
             atomicAdd(a.dacc + r, g.x * pv[v].y - g.y * pv[v].x);   // Im(conj(g) p1)
         }
     }
@@ -650,9 +678,7 @@ cudaError_t launch_pass2(const FloatDev &d, cudaStream_t st) {
     size_t regA = (std::max((size_t)8 * d.m, (size_t)8 * F::xbuf_elems()) + 15) & ~(size_t)15;
     size_t sm = regA + (SINC ? kTabShorts * 2 : 0);
     auto fn = k_fl_pass2_fft<L, E, SINC>;
-    if constexpr (!SINC) {
-        if (d.pk_out) fn = k_fl_pass2_fft<L, E, false, true>;
-    }
+    if (d.pk_out) fn = k_fl_pass2_fft<L, E, SINC, true>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     fn<<<d.npad, (1 << L) / E, sm, st>>>(p);
@@ -828,9 +854,11 @@ cudaError_t launch_af_range(const FloatDev &d, cudaStream_t st) {
 template <int L>
 cudaError_t launch_af_cross(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, Cfg<L>::E>;
-    AfCrossArgs p{d.af_zadj, d.p1, d.af_pk, d.ham_m64, d.ham_n64, d.twm, d.af_dacc, d.m, d.n, d.mpad, d.window};
-    const size_t sm = (size_t)8 * F::xbuf_elems() + (size_t)4 * ((d.m + 15) & ~15);   // pk: whole groups of 16
-    auto fn = k_af_cross_adjoint<L, Cfg<L>::E>;
+    AfCrossArgs p{d.af_zadj, d.p1, d.af_pk, d.ham_m64, d.ham_n64, d.kr, d.tan_s, d.tabq, d.twm, d.af_dacc,
+                  d.m, d.n, d.mpad, d.window};
+    // exchange buffer, packed brackets (whole groups of 16), sinc table
+    const size_t sm = (size_t)8 * F::xbuf_elems() + (size_t)4 * ((d.m + 15) & ~15) + (d.az_sinc ? kTabShorts * 2 : 0);
+    auto fn = d.az_sinc ? k_af_cross_adjoint<L, Cfg<L>::E, true> : k_af_cross_adjoint<L, Cfg<L>::E, false>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     fn<<<d.n, Cfg<L>::T, sm, st>>>(p);
@@ -869,7 +897,7 @@ cudaError_t af_cross(const FloatDev &d, cudaStream_t st) {
 }
 #undef PFA_DISPATCH_L
 
-// Entropy and its gradient w.r.t. the per-pulse phase correction theta (float32, lerp passes).
+// Entropy and its gradient w.r.t. the per-pulse phase correction theta (float32; lerp or float sinc passes).
 cudaError_t autofocus_grad(const FloatDev &d0, const float2 *sig, const float *theta, float *dtheta, double *ent,
                            cudaStream_t st, StageProf *prof) {
     StageProf none;
@@ -884,13 +912,15 @@ cudaError_t autofocus_grad(const FloatDev &d0, const float2 *sig, const float *t
     if ((e = cudaMemsetAsync(d.af_acc, 0, 2 * sizeof(double), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(d.af_dacc, 0, sizeof(float) * d.mpad, st)) != cudaSuccess) return e;
     FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabq, theta, d.p1, d.m, d.n, d.mpad};
-    dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + f1_bins(false) - 1) / f1_bins(false));
-    e = cudaFuncSetAttribute(k_fl_pass1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1_smem(false));
+    const bool rs = d.range_sinc != 0;
+    dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + f1_bins(rs) - 1) / f1_bins(rs));
+    auto k1 = rs ? k_fl_pass1<true> : k_fl_pass1<false>;
+    e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1_smem(rs));
     if (e != cudaSuccess) return e;
-    k_fl_pass1<false><<<g1, 256, f1_smem(false), st>>>(p1);
+    k1<<<g1, 256, f1_smem(rs), st>>>(p1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = pf.mark(st, "pass1_phase")) != cudaSuccess) return e;
-    if ((e = dispatch_pass2<false>(d, st)) != cudaSuccess) return e;
+    if ((e = (d.az_sinc ? dispatch_pass2<true>(d, st) : dispatch_pass2<false>(d, st))) != cudaSuccess) return e;
     if ((e = pf.mark(st, "pass2_win_fft1")) != cudaSuccess) return e;
     if ((e = af_range(d, st)) != cudaSuccess) return e;
     if ((e = pf.mark(st, "range_entropy_adjoint")) != cudaSuccess) return e;
@@ -936,8 +966,6 @@ pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *job) {
         const int r = job->order[i];
         if (r < 0 || r >= m || seen[r]++) return ffail(p, PFA_ERR_BAD_ARG, "order is not a permutation");
     }
-    d.kr_positive = 1;
-    for (int j = 0; j < n; ++j) if (!(job->kr_grid[j] > 0.0)) d.kr_positive = 0;
     d.sgn = job->sgn < 0 ? -1 : 1;
     d.layout = job->layout;
     d.window = (job->ham_m && job->ham_n) ? 1 : 0;
@@ -1043,8 +1071,6 @@ pfa_status pfa_autofocus_grad(pfa_plan *p, const float *sig_dev, const float *th
     if (p->cfg.mode != PFA_MODE_FLOAT32 && p->cfg.mode != PFA_MODE_MIXED) return ffail(p, PFA_ERR_BAD_CONFIG, "plan is not float mode");
     if (!p->job_ready) return ffail(p, PFA_ERR_NOT_READY, "pfa_set_float_job not called");
     pfa::FloatDev &d = p->fl;
-    if (d.range_sinc || d.az_sinc) return ffail(p, PFA_ERR_BAD_CONFIG, "autofocus gradient supports the lerp resampler");
-    if (!d.kr_positive) return ffail(p, PFA_ERR_BAD_CONFIG, "autofocus gradient needs positive KR (ascending pass-2 sources)");
     if (reinterpret_cast<uintptr_t>(sig_dev) & 7) return ffail(p, PFA_ERR_BAD_ARG, "signal must be 8-byte aligned");
     DevGuard dg(p->device);
     cudaError_t e;

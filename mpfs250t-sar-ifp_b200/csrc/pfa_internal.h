@@ -45,13 +45,12 @@ struct FloatDev {
     int window = 1;
     float2 *p1 = nullptr;              // [n][mpad] pass-1 output (range-bin rows, sorted pulses)
     float2 *y1 = nullptr;              // [m2][npad] cross FFT output, transposed (cross-bin rows)
-    int kr_positive = 0;               // KR > 0 everywhere (ascending pass-2 sources)
     int ept_cross = 0, ept_range = 0;    // FFT register tile (complex values per thread; 0 = automatic)
     float2 *af_zadj = nullptr;         // [n][m2] autofocus: adjoint of the range FFT (range-bin rows)
     double *af_acc = nullptr;          // [2] sum I, sum I log I
     float *af_dacc = nullptr;          // [mpad] per-slot gradient accumulators
     uint32_t *af_pk = nullptr;         // [n][m] autofocus: packed pass-2 brackets of the forward pass
-    uint32_t *pk_out = nullptr;        // where the lerp pass 2 stores its packed brackets (or nullptr)
+    uint32_t *pk_out = nullptr;        // where pass 2 stores its packed brackets for the adjoint (or nullptr)
     // split-precision (mixed) mode: tensor-core FFTs for lines of 2048..8192 points
     int mixed = 0;
     uint4 *mx_f128 = nullptr;          // F_128 TMEM image [128 lanes][256 columns] of fp16 pairs

@@ -4,7 +4,8 @@ The reference has no autofocus; this restates the objective the B200 engine diff
 the reference's float PFA (src/form_image_pfa.py:165-246):
 
     x[i, k] = s[i, k] exp(-j theta_i)                      per-pulse phase correction
-    z       = FFT2( W * R2( R1(x) ) )                      R1/R2: the two np.interp passes as sparse
+    z       = FFT2( W * R2( R1(x) ) )                      R1/R2: the two np.interp passes (or the float
+                                                           32-tap sinc of oracle.float_pfa) as sparse
                                                            matrices, W: float64 Hamming product, pad
                                                            to pow2 (natural layout; |z| is invariant to
                                                            the reference's fftshift centring)
@@ -32,15 +33,39 @@ def _interp_matrix(x, xp):
     return (np.concatenate([rows, rows]), np.concatenate([kk, kk + 1]), np.concatenate([1.0 - ff, ff]))
 
 
-def operators(tables):
-    """Per-pulse pass-1 operators and per-range-bin pass-2 operators of resample_kspace."""
+def _sinc_matrix(x, xp):
+    """(rows, cols, vals) of the float 32-tap sinc resample of oracle.float_pfa._interp_sinc (ascending xp):
+    interior brackets (15 <= k <= n-17) take tab[phase][t] / 32768 at k - 15 + t, the others the lerp."""
+    from . import fixed_emulator as fe
+    tab = fe._tab().astype(np.float64) / 32768.0
+    n = xp.size
+    k = np.searchsorted(xp, x, side="right") - 1
+    live = (x >= xp[0]) & (x <= xp[-1])
+    k = np.clip(k, 0, n - 2)
+    f = (x - xp[k]) / (xp[k + 1] - xp[k])
+    ph = np.clip(np.round(np.where(live, f, 0.0) * 32768.0), 0, 32767).astype(np.int64) >> 7
+    interior = live & (k >= 15) & (k <= n - 17)
+    edge = live & ~interior
+    ri = np.nonzero(interior)[0]
+    re_ = np.nonzero(edge)[0]
+    rows = [np.repeat(ri, 32), re_, re_]
+    cols = [(k[ri, None] - 15 + np.arange(32)[None, :]).ravel(), k[re_], k[re_] + 1]
+    vals = [tab[ph[ri]].ravel(), 1.0 - f[re_], f[re_]]
+    return np.concatenate(rows), np.concatenate(cols), np.concatenate(vals)
+
+
+def operators(tables, range_interp="lerp", az_interp="lerp"):
+    """Per-pulse pass-1 operators and per-range-bin pass-2 operators of resample_kspace ("lerp": np.interp,
+    "sinc": the float 32-tap sinc).  A descending source axis is resampled on its ascending view."""
     g = fp.geometry(tables["freq"], tables["ax"], tables["ay"])
     m, n = g["m"], g["n"]
+    op1 = _sinc_matrix if range_interp == "sinc" else _interp_matrix
+    op2 = _sinc_matrix if az_interp == "sinc" else _interp_matrix
     p1 = []
     for i in range(m):
         xp = g["kr"][i]
         rev = xp[0] > xp[-1]
-        r, c, v = _interp_matrix(g["KR"], xp[::-1] if rev else xp)
+        r, c, v = op1(g["KR"], xp[::-1] if rev else xp)
         if rev:
             c = n - 1 - c
         p1.append((r, c, v))
@@ -49,7 +74,7 @@ def operators(tables):
     for j in range(n):
         src = g["KR"][j] * tan_s
         rev = src[0] > src[-1]
-        r, c, v = _interp_matrix(g["KC"], src[::-1] if rev else src)
+        r, c, v = op2(g["KC"], src[::-1] if rev else src)
         if rev:
             c = m - 1 - c
         p2.append((r, c, v))
@@ -88,9 +113,9 @@ def _forward_torch(sig, theta, g, p1, p2, torch):
     return -plogp.sum()
 
 
-def entropy_and_grad(sig, tables, theta):
+def entropy_and_grad(sig, tables, theta, range_interp="lerp", az_interp="lerp"):
     import torch
-    g, p1, p2 = operators(tables)
+    g, p1, p2 = operators(tables, range_interp, az_interp)
     th = torch.tensor(np.asarray(theta, np.float64), requires_grad=True)
     e = _forward_torch(sig, th, g, p1, p2, torch)
     e.backward()
@@ -104,9 +129,9 @@ def entropy(sig, tables, theta, ops=None):
         return float(_forward_torch(sig, torch.tensor(np.asarray(theta, np.float64)), g, p1, p2, torch).item())
 
 
-def fd_grad(sig, tables, theta, idx, h=1e-4):
+def fd_grad(sig, tables, theta, idx, h=1e-4, range_interp="lerp", az_interp="lerp"):
     """Central differences of the float64 entropy w.r.t. theta[idx]."""
-    ops = operators(tables)
+    ops = operators(tables, range_interp, az_interp)
     out = []
     for i in idx:
         tp = np.array(theta, np.float64)

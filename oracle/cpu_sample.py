@@ -12,6 +12,10 @@ stage of one frame, and scales each stage to the full frame:
   detect           S of the G rows                   -> x G/S
 
 The sampled lines are split over ``workers`` spawned processes (one chunk each) when workers > 1.
+
+``fixed_frame_full`` runs the WHOLE frame instead (every pulse, row and column of every stage), with
+each stage's lines split over the spawned workers and int16 planes passed between stages, and returns
+the uint16 image with its timing: the reference arm's timed step.
 """
 from __future__ import annotations
 
@@ -69,6 +73,118 @@ def _detect_chunk(args):
     t = time.perf_counter()
     fe.detect_q(xr, xi)
     return time.perf_counter() - t
+
+
+def _full_p1(args):
+    sr, si, geo, rows, mode = args          # int16 planes of the chunk's pulses, in `rows` order
+    n = geo["n"]
+    out_r = np.empty((len(rows), geo["grid"]), np.int16)
+    out_i = np.empty_like(out_r)
+    for r, i in enumerate(rows):
+        idx, wq = fe.bracket_q15(geo["KRp"], fe.pass1_coords(geo, i))
+        a, b = fe._gather(mode, sr[r].astype(np.int64), si[r].astype(np.int64), idx, wq, n, True)
+        out_r[r], out_i[r] = a, b
+    return out_r, out_i
+
+
+def _full_p2(args):
+    tr, ti, geo, rows, mode = args          # int16 range-bin rows of the corner-turned scratch, [:, :m]
+    m, n, G = geo["m"], geo["n"], geo["grid"]
+    hr = fe.hamming_q15(n, G)
+    hc = fe.hamming_q15(m, G)
+    out_r = np.empty((len(rows), G), np.int16)
+    out_i = np.empty_like(out_r)
+    for r, j in enumerate(rows):
+        src = geo["KRp"][j] * geo["tan_s"]
+        idx, wq = fe.bracket_q15(geo["KCp"], src)
+        a, b = fe._gather(mode, tr[r].astype(np.int64), ti[r].astype(np.int64), idx, wq, m, False)
+        cw = fe.wrap16((hr[j] * hc) >> 15)                       # window_fixed, row j
+        out_r[r] = fe.sat16(fe.wrap16((a * cw) >> 15))
+        out_i[r] = fe.sat16(fe.wrap16((b * cw) >> 15))
+    return out_r, out_i
+
+
+def _full_fft(args):
+    xr, xi = args
+    yr, yi, e = fe.fft_bfp_rows(xr.astype(np.int64), xi.astype(np.int64))
+    return yr.astype(np.int16), yi.astype(np.int16), e
+
+
+def _full_detect(args):
+    yr, yi, sh = args                       # FFT-2 rows (cross bins) and their renorm shifts
+    return fe.detect_q(fe.sat16(yr.astype(np.int64) >> sh[:, None]), fe.sat16(yi.astype(np.int64) >> sh[:, None]))
+
+
+def fixed_frame_full(signal, tables, grid, range_sinc=True, az_sinc=True, workers=1, pool=None):
+    """One whole fixed-point frame of the oracle (``fixed_emulator.form_image``'s stages, every line),
+    each stage split over ``workers`` spawned processes.  Returns (uint16 image [range][cross], dict of
+    stage seconds).  The per-line arithmetic is the oracle's; int16 planes carry the stage outputs
+    between processes (every stage output is saturated to int16)."""
+    stage = {}
+    rmode = "sinc" if range_sinc else "lerp"
+    amode = "sinc" if az_sinc else "lerp"
+    t = time.perf_counter()
+    sr, si, _ = fe.quantize_q0(np.asarray(signal, np.complex64))
+    sr, si = sr.astype(np.int16), si.astype(np.int16)
+    stage["q0"] = time.perf_counter() - t
+    geo = fe.fixed_geometry(tables, grid)
+    m, n, G = geo["m"], geo["n"], grid
+    own = False
+    ex = pool
+    if workers > 1 and ex is None:
+        ex, own = make_pool(workers), True
+    mapper = ex.map if workers > 1 else map
+
+    def chunks(count):
+        return [c for c in np.array_split(np.arange(count), max(1, 2 * workers)) if len(c)]
+
+    try:
+        t = time.perf_counter()
+        s1r = np.zeros((G, G), np.int16)
+        s1i = np.zeros((G, G), np.int16)
+        cs = chunks(m)
+        for c, (a, b) in zip(cs, mapper(_full_p1, [(sr[c], si[c], geo, c, rmode) for c in cs])):
+            s1r[geo["inv_order"][c]] = a
+            s1i[geo["inv_order"][c]] = b
+        stage["pass1"] = time.perf_counter() - t
+        t = time.perf_counter()
+        tr = np.ascontiguousarray(s1r.T[:, :m])
+        ti = np.ascontiguousarray(s1i.T[:, :m])
+        wr = np.empty((G, G), np.int16)
+        wi = np.empty((G, G), np.int16)
+        cs = chunks(G)
+        for c, (a, b) in zip(cs, mapper(_full_p2, [(tr[c], ti[c], geo, c, amode) for c in cs])):
+            wr[c], wi[c] = a, b
+        stage["pass2_window"] = time.perf_counter() - t
+
+        def fft_pass(xr, xi):
+            yr = np.empty_like(xr)
+            yi = np.empty_like(xi)
+            e = np.empty(xr.shape[0], np.int64)
+            for c, (a, b, ee) in zip(cs, mapper(_full_fft, [(xr[c], xi[c]) for c in cs])):
+                yr[c], yi[c], e[c] = a, b, ee
+            return yr, yi, e
+
+        t = time.perf_counter()
+        y1r, y1i, e1 = fft_pass(wr, wi)
+        sh = (int(e1.max()) - e1)[:, None]
+        y1r = fe.sat16(y1r.astype(np.int64) >> sh).astype(np.int16)
+        y1i = fe.sat16(y1i.astype(np.int64) >> sh).astype(np.int16)
+        stage["fft1"] = time.perf_counter() - t
+        t = time.perf_counter()
+        y2r, y2i, e2 = fft_pass(np.ascontiguousarray(y1r.T), np.ascontiguousarray(y1i.T))
+        stage["fft2"] = time.perf_counter() - t
+        t = time.perf_counter()
+        sh2 = int(e2.max()) - e2
+        det = np.empty((G, G), np.uint16)
+        for c, d in zip(cs, mapper(_full_detect, [(y2r[c], y2i[c], sh2[c]) for c in cs])):
+            det[c] = d
+        img = np.ascontiguousarray(det.T)
+        stage["detect"] = time.perf_counter() - t
+    finally:
+        if own:
+            ex.shutdown()
+    return img, {k: round(v, 4) for k, v in stage.items()}
 
 
 def make_pool(workers: int):
@@ -210,3 +326,49 @@ def float_frame_estimate(signal, tables, sample=64, workers=1, pool=None, seed=0
     return dict(ms_per_frame=1000.0 * total, stage_seconds={k: round(v, 4) for k, v in stage.items()},
                 sample=f"{s1} of {m} pulses, {s2} of {n} range bins, {fr.shape[0]} of {m2} FFT rows and "
                        f"{fc.shape[0]} of {n2} FFT columns, scaled to the full frame", workers=workers)
+
+
+# ----------------------------------------------------------------------------- C restatement
+_CLIB = None
+
+
+def _c_oracle():
+    """ctypes handle of oracle/lib/libfixed_oracle.so (built by oracle/Makefile)."""
+    global _CLIB
+    if _CLIB is None:
+        import ctypes as C
+        from pathlib import Path
+        path = Path(__file__).resolve().parent / "lib" / "libfixed_oracle.so"
+        if not path.is_file():
+            raise RuntimeError(f"{path} not built: run `make -C oracle`")
+        lib = C.CDLL(str(path))
+        P = C.c_void_p
+        lib.pfa_oracle_fixed_frame.restype = C.c_int
+        lib.pfa_oracle_fixed_frame.argtypes = [P, C.c_int, C.c_int, C.c_int] + [P] * 12 + [C.c_int] * 3 + [P] * 4
+        _CLIB = lib
+    return _CLIB
+
+
+def c_fixed_frame(signal, tables, grid, range_sinc=True, az_sinc=True, threads=0):
+    """One whole fixed-point frame of the C restatement (oracle/fixed_frame.c) on ``threads`` host threads
+    (0 = all).  Returns (uint16 image [range][cross], dict(q0_exp, e_range, e_az))."""
+    import ctypes as C
+    lib = _c_oracle()
+    sig = np.ascontiguousarray(signal, np.complex64)
+    m, n = sig.shape
+    geo = fe.fixed_geometry(tables, grid)
+    wr, wi = fe.twiddles_q15(grid)
+    arrs = [np.ascontiguousarray(a) for a in (
+        geo["f0"], geo["df"], geo["fac"], np.asarray(geo["inv_order"], np.int32), geo["tan_s"], geo["KRp"],
+        geo["KCp"], fe.hamming_q15(n, grid).astype(np.int32), fe.hamming_q15(m, grid).astype(np.int32),
+        wr.astype(np.int32), wi.astype(np.int32), fe._tab().astype(np.int16))]
+    img = np.empty((grid, grid), np.uint16)
+    e1 = np.empty(grid, np.int32)
+    e2 = np.empty(grid, np.int32)
+    q0 = np.zeros(1, np.int32)
+    ptr = lambda a: C.c_void_p(a.ctypes.data)   # noqa: E731
+    st = lib.pfa_oracle_fixed_frame(ptr(sig), m, n, grid, *[ptr(a) for a in arrs], int(bool(range_sinc)),
+                                    int(bool(az_sinc)), int(threads), ptr(img), ptr(e1), ptr(e2), ptr(q0))
+    if st != 0:
+        raise MemoryError("C oracle: host allocation failed")
+    return img, dict(q0_exp=int(q0[0]), e_range=e1, e_az=e2)

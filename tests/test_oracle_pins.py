@@ -164,3 +164,34 @@ def test_synth_phase_error_matches_autofocus_oracle():
     from oracle import autofocus_ref
     for m, seed in ((4096, 4), (256, 7)):
         assert np.array_equal(synth.phase_error(m, seed=seed), autofocus_ref.phase_error(m, seed=seed))
+
+
+def test_c_restatement_matches_numpy_oracle():
+    """The C restatement of the fixed datapath (oracle/fixed_frame.c, timed by bench.py's reference arm)
+    gives the NumPy oracle's image and exponents on every interpolator pair and a descending axis."""
+    from oracle import cpu_sample
+    from pfa_b200 import geometry, synth
+    for m, n, grid, rs, az, seed in [(300, 250, 512, False, True, 42), (240, 256, 256, True, False, 3),
+                                     (120, 110, 128, True, True, 7), (200, 180, 256, False, False, 11)]:
+        sc = synth.make_scene(m, n, n_targets=12, clutter_db=-10.0, seed=seed, jitter=0.3)
+        tb = geometry.prepare_tables_from_scene(sc)
+        ref, d = fe.form_image(sc.signal, tb, grid, rs, az)
+        img, dc = cpu_sample.c_fixed_frame(sc.signal, tb, grid, rs, az, threads=2)
+        assert np.array_equal(img, ref), (m, n, grid, rs, az)
+        assert dc["q0_exp"] == d["q0_exp"]
+        assert np.array_equal(dc["e_range"], d["e_range"]) and np.array_equal(dc["e_az"], d["e_az"])
+
+
+def test_c_restatement_reproduces_reference_crc_of_full_frame():
+    r"""The whole Centerfield-shaped 5634x4319 -> 8192^2 sinc/sinc frame: the C restatement's image has the
+    CRC the unmodified reference emulator produced (tests/golden/big_frames.json)."""
+    import json
+    from oracle import cpu_sample
+    from pfa_b200 import geometry, synth
+    from pathlib import Path
+    case = json.loads((Path(__file__).parent / "golden" / "big_frames.json").read_text())["cases"]["centerfield_5634x4319_sinc"]
+    sc = synth.workload_scene("centerfield_5634x4319")
+    assert _crc(sc.signal) == case["input_crc"]
+    tb = geometry.prepare_tables_from_scene(sc)
+    img, _ = cpu_sample.c_fixed_frame(sc.signal, tb, 8192, True, True)
+    assert fe.frame_crc(img) == case["image_crc"]
