@@ -339,8 +339,9 @@ def measure_modes(a, local):
 
 def measure_batch(a, local, nscene=16, af_iters=5, streams=4):
     """16 scenes with pulses and samples uniform in [2048, 8192] (seed 5), 64-512 targets + clutter, each
-    formed on its own pow2 raster after `af_iters` autofocus steps, autotuned FFT tiles; one CUDA graph
-    launch for the batch vs one scene at a time on one stream.  Aggregate frames/s."""
+    formed on its own pow2 raster after `af_iters` autofocus steps on the device (pfa_autofocus_step; the
+    image applies the phase in pass 1), autotuned FFT tiles; one CUDA graph launch for the batch vs one
+    scene at a time on one stream.  Aggregate frames/s."""
     import numpy as np
     import torch
     from pfa_b200 import autotune, batch, geometry, synth
@@ -357,7 +358,7 @@ def measure_batch(a, local, nscene=16, af_iters=5, streams=4):
     reps = max(2, min(a.steps, 5))
     shapes = [list(map(int, s.shape)) for _, s in scenes]
     out = {"workload": f"{nscene} scenes, M,N uniform in [2048, 8192] (seed 5), 64-512 targets + clutter, "
-                       f"pow2 rasters, {af_iters} autofocus iterations each (FP32 gradients)",
+                       f"pow2 rasters, {af_iters} autofocus iterations each on the device (FP32 gradients)",
            "shapes": shapes, "tiles": [list(t) for t in tiles], "streams": streams}
     for tag, mixed in (("fp32", False), ("mixed", True)):
         bf = batch.BatchFormer(scenes, streams=streams, tiles=tiles, af_iters=af_iters, device=local, mixed=mixed)

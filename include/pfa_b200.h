@@ -193,10 +193,11 @@ pfa_status pfa_form_float(pfa_plan *plan, const float *sig_dev, void *out_dev, i
 pfa_status pfa_form_float_host(pfa_plan *plan, const float *sig_host, void *out_host, int32_t detect);
 
 /* Image-entropy autofocus.  For the per-pulse phase correction theta[m] (float32, device) the plan
- * forms the float image of s[i,k] exp(-j theta_i) (lerp passes, window as set, natural layout), its
+ * forms the float image of s[i,k] exp(-j theta_i) (the plan's lerp or float-sinc passes, window as set,
+ * natural layout), its
  * entropy E = -sum p log p with p = |z|^2 / sum |z|^2, and dE/dtheta[m] with hand-written adjoint
- * kernels (range FFT recomputed, adjoint FFTs, window, transposed pass-2 resample as an atomics-free
- * segmented reduction).  entropy_dev (double, device) may be NULL.  The first call on a plan adds its
+ * kernels (range FFT recomputed, adjoint FFTs, window, transposed pass-2 resample -- lerp or 32-tap sinc --
+ * as an atomics-free segmented reduction; descending source axes included).  entropy_dev (double, device) may be NULL.  The first call on a plan adds its
  * gradient workspace to the plan (12 n pow2(m) bytes at most: the range-FFT adjoint and the packed
  * pass-2 brackets), held until pfa_plan_destroy and not counted by pfa_plan_workspace_bytes.  The
  * reference has no autofocus; the image it forms is form_image_pfa.pfa (src/form_image_pfa.py:243-246). */
@@ -215,6 +216,20 @@ pfa_status pfa_autofocus_grad(pfa_plan *plan, const float *sig_dev, const float 
 size_t pfa_display_workspace_bytes(void);
 pfa_status pfa_display_u8(const float *mag_dev, int64_t count, float percentile, void *workspace_dev, uint8_t *out_dev,
                           float *hi_dev, void *stream);
+
+/* Float frame of the phase-corrected signal s[i,k] exp(-j theta_i) (theta: float32 [m], device): the
+ * correction is applied in pass 1, where it commutes with the per-pulse resample, so no corrected copy
+ * of the signal is made.  Same outputs and rules as pfa_form_float; the image autofocus converges to. */
+pfa_status pfa_form_float_phase(pfa_plan *plan, const float *sig_dev, const float *theta_dev, void *out_dev,
+                                int32_t detect, void *stream);
+
+/* One autofocus descent step on the device: the entropy gradient g of pfa_autofocus_grad, then
+ * theta <- theta - step (g - mean g) / max |g - mean g| in place (the update pfa_b200.autofocus.autofocus
+ * applies; a constant phase does not change the image).  theta_dev: float32 [m], device; entropy_dev
+ * (double, device) may be NULL.  Stream-ordered, no host synchronisation: a loop of steps can be
+ * captured in one CUDA graph. */
+pfa_status pfa_autofocus_step(pfa_plan *plan, const float *sig_dev, float *theta_dev, float step, double *entropy_dev,
+                              void *stream);
 
 /* Per-stage device timing, the counterpart of the board's per-stage timestamps sar_stage_ts[]
  * (sar_sequencer.c:235-238) and form_image_pfa.StepTimer (src/form_image_pfa.py:42-60).  When enabled,

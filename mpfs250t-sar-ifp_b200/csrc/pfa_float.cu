@@ -658,8 +658,43 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
 
 __global__ void k_af_finish(const float *dacc, const int32_t *order, const double *acc, float *dtheta, double *ent, int m) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < m) dtheta[order[r]] = 2.0f * dacc[r];
+    if (r < m && dtheta) dtheta[order[r]] = 2.0f * dacc[r];
     if (r == 0 && ent) ent[0] = log(acc[0]) - acc[1] / acc[0];
+}
+
+// One step of the autofocus descent on the device: g = dE/dtheta (2 dacc in slot order), theta <- theta -
+// step (g - mean g) / max |g - mean g| (a constant phase does not change the image).  One block.
+__global__ void __launch_bounds__(1024) k_af_update(const float *dacc, const int32_t *order, float *theta, int m,
+                                                    float step) {
+    __shared__ double red[32];
+    __shared__ float bc[2];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double s = 0.0;
+    for (int r = tid; r < m; r += blockDim.x) s += 2.0 * (double)dacc[r];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        bc[0] = (float)(t / m);
+    }
+    __syncthreads();
+    const float mean = bc[0];
+    float mx = 0.f;
+    for (int r = tid; r < m; r += blockDim.x) mx = fmaxf(mx, fabsf(2.0f * dacc[r] - mean));
+    mx = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(mx)));   // non-negative floats
+    if (lane == 0) red[warp] = mx;
+    __syncthreads();
+    if (tid == 0) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = fmaxf(t, (float)red[w]);
+        bc[1] = fmaxf(t, 1e-30f);
+    }
+    __syncthreads();
+    const float scale = step / bc[1];
+    for (int r = tid; r < m; r += blockDim.x) theta[order[r]] -= scale * (2.0f * dacc[r] - mean);
 }
 
 // ------------------------------------------------------------------------------------------ launch
@@ -804,13 +839,14 @@ void float_free(FloatDev &d) {
     mixed_free(d);
 }
 
-cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int detect, cudaStream_t st, StageProf *prof) {
+cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int detect, cudaStream_t st, StageProf *prof,
+                       const float *theta) {
     StageProf none;
     StageProf &pf = prof ? *prof : none;
     pf.count = 0;
     cudaError_t e = pf.mark(st, "start");
     if (e != cudaSuccess) return e;
-    FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabq, nullptr, d.p1, d.m, d.n, d.mpad};
+    FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabq, theta, d.p1, d.m, d.n, d.mpad};
     dim3 g1((d.m + F1_SLOTS - 1) / F1_SLOTS, (d.n + f1_bins(d.range_sinc) - 1) / f1_bins(d.range_sinc));
     if (d.range_sinc) {
         e = cudaFuncSetAttribute(k_fl_pass1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f1_smem(true));
@@ -1065,9 +1101,45 @@ pfa_status pfa_form_float_host_frames(pfa_plan *p, const float *const *sig_hosts
     return st != PFA_OK ? st : mixed_timeout_check(p);
 }
 
+pfa_status pfa_form_float_phase(pfa_plan *p, const float *sig_dev, const float *theta_dev, void *out_dev, int32_t detect,
+                                void *stream) {
+    if (!p || !sig_dev || !theta_dev || !out_dev) return PFA_ERR_BAD_ARG;
+    if (p->cfg.mode != PFA_MODE_FLOAT32 && p->cfg.mode != PFA_MODE_MIXED) return ffail(p, PFA_ERR_BAD_CONFIG, "plan is not float mode");
+    if (!p->job_ready) return ffail(p, PFA_ERR_NOT_READY, "pfa_set_float_job not called");
+    if (detect < PFA_DETECT_MAG || detect > PFA_DETECT_COMPLEX) return ffail(p, PFA_ERR_BAD_ARG, "bad detect mode");
+    if (reinterpret_cast<uintptr_t>(sig_dev) & 7) return ffail(p, PFA_ERR_BAD_ARG, "signal must be 8-byte aligned");
+    if (p->fl.mixed && (reinterpret_cast<uintptr_t>(out_dev) & 15))
+        return ffail(p, PFA_ERR_BAD_ARG, "mixed mode: output must be 16-byte aligned");
+    DevGuard dg(p->device);
+    cudaError_t e = pfa::float_form(p->fl, reinterpret_cast<const float2 *>(sig_dev), out_dev, detect,
+                                    reinterpret_cast<cudaStream_t>(stream), &p->prof, theta_dev);
+    if (e != cudaSuccess) return fcuda(p, e, "float form");
+    return PFA_OK;
+}
+
+static pfa_status autofocus_common(pfa_plan *p, const float *sig_dev, const float *theta_dev, float *dtheta_dev,
+                                   double *entropy_dev, void *stream);
+
+pfa_status pfa_autofocus_step(pfa_plan *p, const float *sig_dev, float *theta_dev, float step, double *entropy_dev,
+                              void *stream) {
+    if (!p || !sig_dev || !theta_dev) return PFA_ERR_BAD_ARG;
+    pfa_status st = autofocus_common(p, sig_dev, theta_dev, nullptr, entropy_dev, stream);
+    if (st != PFA_OK) return st;
+    DevGuard dg(p->device);
+    pfa::k_af_update<<<1, 1024, 0, reinterpret_cast<cudaStream_t>(stream)>>>(p->fl.af_dacc, p->fl.order, theta_dev,
+                                                                               p->fl.m, step);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PFA_OK : fcuda(p, e, "autofocus update");
+}
+
 pfa_status pfa_autofocus_grad(pfa_plan *p, const float *sig_dev, const float *theta_dev, float *dtheta_dev,
                               double *entropy_dev, void *stream) {
     if (!p || !sig_dev || !theta_dev || !dtheta_dev) return PFA_ERR_BAD_ARG;
+    return autofocus_common(p, sig_dev, theta_dev, dtheta_dev, entropy_dev, stream);
+}
+
+static pfa_status autofocus_common(pfa_plan *p, const float *sig_dev, const float *theta_dev, float *dtheta_dev,
+                                   double *entropy_dev, void *stream) {
     if (p->cfg.mode != PFA_MODE_FLOAT32 && p->cfg.mode != PFA_MODE_MIXED) return ffail(p, PFA_ERR_BAD_CONFIG, "plan is not float mode");
     if (!p->job_ready) return ffail(p, PFA_ERR_NOT_READY, "pfa_set_float_job not called");
     pfa::FloatDev &d = p->fl;

@@ -107,8 +107,9 @@ size_t fixed_workspace_bytes(int m, int n, int G);
 cudaError_t fixed_alloc(FixedDev &d, int m, int n, int G);
 void fixed_free(FixedDev &d);
 
+// theta (device, [m], or nullptr): per-pulse phase correction exp(-j theta_i) applied in pass 1
 cudaError_t float_form(const FloatDev &d, const float2 *sig, void *out, int detect, cudaStream_t st,
-                       StageProf *prof);
+                       StageProf *prof, const float *theta = nullptr);
 size_t float_workspace_bytes(int m, int n);
 cudaError_t float_alloc(FloatDev &d, int m, int n);
 void float_free(FloatDev &d);

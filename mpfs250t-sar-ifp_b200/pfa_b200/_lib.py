@@ -67,6 +67,8 @@ SIGNATURES = {
     "pfa_form_fixed_host_frames": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
     "pfa_form_float_host_frames": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
     "pfa_autofocus_grad":(C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pfa_autofocus_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p]),
+    "pfa_form_float_phase": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "pfa_display_workspace_bytes": (C.c_size_t, []),
     "pfa_display_u8": (C.c_int, [C.c_void_p, C.c_int64, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "pfa_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),

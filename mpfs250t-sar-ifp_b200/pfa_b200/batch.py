@@ -5,8 +5,10 @@ to ``streams`` CUDA streams largest-first (greedy on the estimated frame cost, s
 together), and captures the whole batch -- for every scene ``af_iters`` autofocus gradient steps on its
 per-pulse phase, the phase-corrected signal and the final detected image -- into one CUDA graph.
 ``replay()`` then forms the whole batch with a single graph launch; kernels of different scenes
-overlap across the streams and fill the GPU that one small scene alone leaves idle.  ``run_eager()``
-is the one-scene-at-a-time reference on a single stream.
+overlap across the streams.  Every node of the graph is a kernel of the engine: the autofocus update runs
+on the device (``pfa_autofocus_step``) and the final image applies the phase correction in pass 1
+(``pfa_form_float_phase``), so the batch has no eager tensor operations and no host round trip.
+``run_eager()`` is the one-scene-at-a-time reference on a single stream.
 """
 from __future__ import annotations
 
@@ -34,9 +36,7 @@ class BatchFormer:
         dev = self.signals[0].device
         self.images = [torch.empty((p.m2, p.n2), dtype=torch.float32, device=dev) for p in self.plans]
         self.theta = [torch.zeros(p.m, dtype=torch.float32, device=dev) for p in self.plans]
-        self.dtheta = [torch.empty_like(t) for t in self.theta]
-        self.ent = [torch.empty((), dtype=torch.float64, device=dev) for _ in self.plans]
-        self.corr = [torch.empty_like(s) for s in self.signals]
+        self.zero = [torch.zeros_like(t) for t in self.theta]
         self.nstreams = max(1, min(int(streams), self.n))
         self.streams = [torch.cuda.Stream(device=dev) for _ in range(self.nstreams)]
         cost = [p.m2 * p.n2 for p in self.plans]
@@ -49,21 +49,15 @@ class BatchFormer:
         self.graph = None
 
     def _scene(self, i, stream):
-        torch = self.torch
         p, sig = self.plans[i], self.signals[i]
-        th, dth, ent = self.theta[i], self.dtheta[i], self.ent[i]
-        th.zero_()
+        th = self.theta[i]
+        th.copy_(self.zero[i])               # a memcpy node: theta starts at 0 on every replay
         for _ in range(self.af_iters):
-            af.entropy_grad(p, sig, th, dth, ent, stream=stream)
-            g = dth - dth.mean()
-            th.sub_(self.af_step * g / g.abs().max().clamp_min(1e-30))
+            af.descent_step(p, sig, th, self.af_step, stream=stream)
         if self.af_iters:
-            rot = torch.polar(torch.ones_like(th), -th).to(torch.complex64)
-            torch.mul(sig, rot[:, None], out=self.corr[i])
-            src = self.corr[i]
+            af.form_corrected(p, sig, th, out=self.images[i], stream=stream)
         else:
-            src = sig
-        p.form(src, out=self.images[i], stream=stream)
+            p.form(sig, out=self.images[i], stream=stream)
 
     def run_eager(self):
         """One scene after another on the current stream (the baseline the graph is compared with)."""

@@ -95,3 +95,28 @@ def test_autograd_function_and_focusing(torch_cuda):
     assert hist[-1] < hist[0]
     e_true = afr.entropy(sig, tb, phi)
     assert hist[-1] <= e_true + 0.1 * (hist[0] - e_true)
+
+
+def test_device_step_and_corrected_form(torch_cuda):
+    """pfa_autofocus_step equals the gradient plus the host-side update; pfa_form_float_phase equals the
+    frame of the corrected signal."""
+    torch = torch_cuda
+    sig, tb, phi = _scene(256, 240, 13)
+    x = torch.from_numpy(sig).cuda()
+    with engine.FloatPlan(256, 240) as plan:
+        plan.set_tables(tb)
+        th0 = torch.from_numpy(np.random.default_rng(13).normal(0.0, 0.2, 256).astype(np.float32)).cuda()
+        _, g = autofocus.entropy_grad(plan, x, th0)
+        g = g - g.mean()
+        want = th0 - 0.3 * g / g.abs().max()
+        got = th0.clone()
+        autofocus.descent_step(plan, x, got, 0.3)
+        assert torch.allclose(got, want, atol=1e-6)
+        img = autofocus.form_corrected(plan, x, got, detect="complex")
+        corr = x * torch.polar(torch.ones_like(got), -got)[:, None]
+        ref = plan.form(corr.contiguous(), detect="complex")
+        assert float(torch.linalg.vector_norm(img - ref) / torch.linalg.vector_norm(ref)) <= 1e-6
+        # the device loop of autofocus() follows the same path as the one with history
+        t_dev, _ = autofocus.autofocus(plan, x, steps=5, step=0.3)
+        t_host, h = autofocus.autofocus(plan, x, steps=5, step=0.3, history=True)
+        assert torch.allclose(t_dev, t_host, atol=1e-4) and len(h) == 5

@@ -141,3 +141,23 @@ def test_mixed_batch_graph(torch_cuda):
         assert fp.rel_l2(b.cpu().numpy(), a.cpu().numpy()) <= 1e-4
     ref.close()
     bf.close()
+
+
+def test_batch_images_against_the_oracle_per_scene(torch_cuda):
+    """After the batch's autofocus iterations (device steps in the graph), every scene's image equals the
+    FP64 oracle's image of the signal corrected by the batch's own final phase (FP32 images: 1e-6;
+    split-precision images: 1e-4)."""
+    torch = torch_cuda
+    shapes = [(300, 400), (520, 260), (2100, 700)]
+    scenes = _scenes(torch, shapes, 95)
+    for mixed, tol in ((False, 1e-6), (True, 1e-4)):
+        bf = batch.BatchFormer(scenes, streams=2, af_iters=3, mixed=mixed)
+        bf.replay()
+        torch.cuda.synchronize()
+        for (tb, x), im, th in zip(scenes, bf.images, bf.theta):
+            t = th.double().cpu().numpy()
+            corr = (x.cpu().numpy() * np.exp(-1j * t)[:, None]).astype(np.complex64)
+            r64 = np.abs(fp.pfa_image(corr, tb["freq"], tb["ax"], tb["ay"], tb["sgn"], precision="f64"))
+            assert fp.rel_l2(im.cpu().numpy(), r64) <= tol, (mixed, tuple(x.shape))
+            assert np.abs(t).max() > 0          # the phase did move
+        bf.close()
