@@ -26,6 +26,19 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <int N>
 __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// Bulk prefetch of `bytes` (16-byte aligned address, size a multiple of 16) into L2, 16 KB per instruction,
+// issued by the first threads of the block: a line kernel prefetches the line of the block that will start
+// when this one ends, so that block's loads find it in L2.
+__device__ __forceinline__ void l2_prefetch(const void *p, size_t bytes, int tid) {
+    constexpr size_t CH = 16384;
+    const size_t off = (size_t)tid * CH;
+    if (off < bytes) {
+        const uint32_t sz = (uint32_t)(bytes - off < CH ? bytes - off : CH);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(static_cast<const char *>(p) + off), "r"(sz)
+                     : "memory");
+    }
+}
+
 // ------------------------------------------------------------------------------------------ brackets
 // np.interp bracket on an ascending accessor xa(0..n-1): returns j with xa(j) <= x < xa(j+1) and the
 // fraction, or -1 when x is outside [xa(0), xa(n-1)]; x == xa(n-1) gives j = n-2, frac = 1.

@@ -78,17 +78,41 @@ __global__ void __launch_bounds__(512) k_disp_hist(const float *__restrict__ v, 
         if (h[i]) atomicAdd(&ws->hist[i], h[i]);
 }
 
-// the bin holding rank `rank`: fixes `width` more bits of the prefix, clears the histogram for the next pass
-__global__ void k_disp_pick(DispWs *ws, int width, int last) {
-    if (threadIdx.x == 0) {
-        DispCtrl &c = ws->ctrl;
-        unsigned long long acc = 0;
-        int b = 0;
-        for (; b < (1 << width) - 1; ++b) {
-            if (acc + ws->hist[b] > c.rank) break;
-            acc += ws->hist[b];
+// the bin holding rank `rank`: fixes `width` more bits of the prefix, clears the histogram for the next pass.
+// One block of 512 threads: each thread scans 4 consecutive bins, a block-wide exclusive scan of the thread
+// sums locates the bin.
+__global__ void __launch_bounds__(512) k_disp_pick(DispWs *ws, int width, int last) {
+    __shared__ unsigned long long part[512];
+    const int tid = threadIdx.x;
+    const int nb = 1 << width;                          // 1024 or 2048 bins: at most 4 per thread
+    unsigned int h[4];
+    unsigned long long s = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int b = 4 * tid + i;
+        h[i] = b < nb ? ws->hist[b] : 0u;
+        s += h[i];
+    }
+    part[tid] = s;
+    __syncthreads();
+    for (int off = 1; off < 512; off <<= 1) {           // inclusive Hillis-Steele scan of the thread sums
+        const unsigned long long v = tid >= off ? part[tid - off] : 0ull;
+        __syncthreads();
+        part[tid] += v;
+        __syncthreads();
+    }
+    const unsigned long long rank = ws->ctrl.rank;
+    const unsigned long long before = tid ? part[tid - 1] : 0ull;
+    if (before <= rank && rank < part[tid]) {           // exactly one thread holds the rank
+        unsigned long long acc = before;
+        int b = 4 * tid;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (acc + h[i] > rank) { b = 4 * tid + i; break; }
+            acc += h[i];
         }
-        c.rank -= acc;
+        DispCtrl &c = ws->ctrl;
+        c.rank = rank - acc;
         c.below += acc;
         c.prefix = (c.prefix << width) | (unsigned int)b;
         if (last) {
@@ -97,7 +121,7 @@ __global__ void k_disp_pick(DispWs *ws, int width, int last) {
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kBins; i += blockDim.x) ws->hist[i] = 0u;
+    for (int i = tid; i < kBins; i += blockDim.x) ws->hist[i] = 0u;
 }
 
 // s[k + 1] when it is larger than s[k]: the smallest value above s[k]

@@ -51,6 +51,17 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// Bulk prefetch of `bytes` (16-byte aligned, a multiple of 16) into L2, 16 KB per instruction by the first
+// threads of the block: a line kernel prefetches the row of the block that starts when this one ends.
+__device__ __forceinline__ void l2_prefetch(const void *p, size_t bytes, int tid) {
+    constexpr size_t CH = 16384;
+    const size_t off = (size_t)tid * CH;
+    if (off < bytes) {
+        const uint32_t sz = (uint32_t)(bytes - off < CH ? bytes - off : CH);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(static_cast<const char *>(p) + off), "r"(sz)
+                     : "memory");
+    }
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // Smallest e with M <= 32767 * 2^e, i.e. ceil(log2(M / 32767)) of fixedpoint.fit_scale for a float32
@@ -592,6 +603,7 @@ struct Pass2Args {
     int32_t *e1, *ctrl;
     int m, n, mpad;
     int cubic;                        // 4-tap Lagrange instead of the lerp (SINC off)
+    int pf;                           // L2 prefetch distance in rows (resident blocks of the grid), 0 = none
 };
 
 template <int L, int E, bool SINC>
@@ -614,6 +626,7 @@ __global__ void __launch_bounds__((1 << L) / E) k_fx_pass2_fft(Pass2Args a) {
     // the twiddles and the sinc table stream in while the p1 row is unpacked into int32 I/Q pairs (one
     // 8-byte shared load per sinc tap, no sign extension in the gather)
     {
+        if (a.pf && j + a.pf < a.n) l2_prefetch(a.p1 + (size_t)(j + a.pf) * a.mpad, (size_t)4 * a.mpad, tid);
         for (int c = tid; c < N / 4; c += T) cp_async16(tw + 4 * c, a.tw + 4 * c);
         if (SINC)
             for (int c = tid; c < 256 * kSincTaps / 8; c += T) cp_async16(tab + 8 * c, a.sinc + 8 * c);
@@ -772,6 +785,18 @@ __global__ void __launch_bounds__(256) k_fx_detect(const uint32_t *__restrict__ 
 }
 
 // ------------------------------------------------------------------------------------------ launch
+// Blocks of `fn` resident on the whole device at once (the L2 prefetch distance of the line kernels).
+template <class K>
+int resident_blocks(K fn, int threads, size_t smem) {
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem) != cudaSuccess) {
+        (void)cudaGetLastError();           // no prefetch; leave no error behind for the launch check
+        return 0;
+    }
+    return sms * per;
+}
+
 template <int L>
 struct FixedLaunch {
     static constexpr int N = 1 << L;
@@ -820,15 +845,17 @@ struct FixedLaunch {
         if ((e = pf.mark(st, "pass1")) != cudaSuccess) return e;
         // K2: pass 2 + window + FFT-1
         Pass2Args p2{d.p1, d.tan_s, d.krp, d.kcp, d.hamr, d.hamc, d.tw, d.sinc, d.y1, d.e1, d.ctrl, d.m, d.n, d.mpad,
-                     d.az_cubic};
+                     d.az_cubic, 0};
         const size_t s2 = pass2_smem(d.m, d.az_sinc != 0);
         if (d.az_sinc) {
             e = cudaFuncSetAttribute(k_fx_pass2_fft<L, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);
             if (e != cudaSuccess) return e;
+            p2.pf = resident_blocks(k_fx_pass2_fft<L, E, true>, T, s2);
             k_fx_pass2_fft<L, E, true><<<d.n, T, s2, st>>>(p2);
         } else {
             e = cudaFuncSetAttribute(k_fx_pass2_fft<L, E, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2);
             if (e != cudaSuccess) return e;
+            p2.pf = resident_blocks(k_fx_pass2_fft<L, E, false>, T, s2);
             k_fx_pass2_fft<L, E, false><<<d.n, T, s2, st>>>(p2);
         }
         if ((e = pf.mark(st, "pass2_win_fft1")) != cudaSuccess) return e;

@@ -388,6 +388,8 @@ struct FFft2Args {
     void *out;
     int n, npad, centred, detect, inverse;
     float scale;
+    int pf;               // L2 prefetch distance in lines (the resident blocks of the grid), 0 = none
+    int nlines;
 };
 
 template <int L, int E>
@@ -398,6 +400,7 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_fl_fft2(FFf
     float2 *xbuf = reinterpret_cast<float2 *>(smem);
     const int tid = threadIdx.x;
     const int k = blockIdx.x;                  // cross bin (row of the output image)
+    if (a.pf && k + a.pf < a.nlines) l2_prefetch(a.y1t + (size_t)(k + a.pf) * a.npad, (size_t)8 * a.npad, tid);
     float2 x[E];
     const float2 *rowk = a.y1t + (size_t)k * a.npad;
 #pragma unroll
@@ -698,6 +701,18 @@ __global__ void __launch_bounds__(1024) k_af_update(const float *dacc, const int
 }
 
 // ------------------------------------------------------------------------------------------ launch
+// Blocks of `fn` resident on the whole device at once (the L2 prefetch distance of the line kernels).
+template <class K>
+int resident_blocks(K fn, int threads, size_t smem) {
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem) != cudaSuccess) {
+        (void)cudaGetLastError();           // no prefetch; leave no error behind for the launch check
+        return 0;
+    }
+    return sms * per;
+}
+
 template <int L>
 struct Cfg {
     static constexpr int N = 1 << L;
@@ -723,11 +738,12 @@ cudaError_t launch_pass2(const FloatDev &d, cudaStream_t st) {
 template <int L, int E>
 cudaError_t launch_fft2(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st) {
     using F = F32Fft<L, E>;
-    FFft2Args p{d.y1, d.twn, out, d.n, d.npad, d.layout == PFA_LAYOUT_CENTRED, detect, d.sgn > 0, scale};
+    FFft2Args p{d.y1, d.twn, out, d.n, d.npad, d.layout == PFA_LAYOUT_CENTRED, detect, d.sgn > 0, scale, 0, d.m2};
     size_t sm = (size_t)8 * F::xbuf_elems();
     auto fn = k_fl_fft2<L, E>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
+    p.pf = resident_blocks(fn, (1 << L) / E, sm);
     fn<<<d.m2, (1 << L) / E, sm, st>>>(p);
     return cudaGetLastError();
 }

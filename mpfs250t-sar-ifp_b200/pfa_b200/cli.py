@@ -9,6 +9,7 @@ with ``--tables`` an .npz of ``prepare_tables`` output).  Prints the device time
 saves the last image.  Modes: ``fixed`` (bit-exact emulator datapath), ``float`` (FP32), ``mixed``
 (split-precision tensor-core FFTs) and ``autofocus`` (the image-entropy gradient w.r.t. the per-pulse
 phase of a scene with the injected quadratic + random-walk phase error; one gradient per frame).
+``--display`` adds the device display scaling of save_detected_geotiff to each float frame.
 """
 from __future__ import annotations
 
@@ -34,6 +35,8 @@ def main(argv=None) -> int:
     ap.add_argument("--tables", help=".npz of prepare_tables output (with --input)")
     ap.add_argument("--out", help="save the last image (.npy)")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--display", action="store_true",
+                    help="float/mixed: also scale each |img| to the uint8 display image on the device")
     a = ap.parse_args(argv)
 
     import torch
@@ -81,7 +84,15 @@ def main(argv=None) -> int:
             img = form()
             e1.record()
             torch.cuda.synchronize()
-            print(f"frame {k}: {e0.elapsed_time(e1):.3f} ms  ({a.mode}, {m}x{n} -> {tuple(img.shape)})")
+            msg = f"frame {k}: {e0.elapsed_time(e1):.3f} ms  ({a.mode}, {m}x{n} -> {tuple(img.shape)})"
+            if a.display and a.mode != "fixed" and a.detect == "mag":
+                from . import geocode
+                e0.record()
+                disp, hi = geocode.display_u8(img)
+                e1.record()
+                torch.cuda.synchronize()
+                msg += f"; display {e0.elapsed_time(e1):.3f} ms (hi {float(hi):.6g})"
+            print(msg)
         if a.out:
             np.save(a.out, img.cpu().numpy())
     return 0
