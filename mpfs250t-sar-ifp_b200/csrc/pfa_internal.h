@@ -57,6 +57,7 @@ struct FloatDev {
     uint4 *mx_fn2m = nullptr, *mx_fn2n = nullptr;   // F_{m2/128}, F_{n2/128} shared-memory images
     int *mx_err = nullptr;             // device flag: a tensor-core completion wait timed out
     int mx_clusters = 0;               // resident 4-CTA clusters of the mixed pass 2
+    int mx_probe = 0;                  // test hook: polls of the range FFT's wait on an unarmed barrier
     int sms = 0;                       // SM count of the plan's device
 };
 

@@ -52,6 +52,7 @@ struct MxFft2Args {
     int *err;
     int n, npad, rows, centred, detect, inverse;
     float scale;
+    int probe;            // test hook: > 0 = polls of a wait on a barrier nothing arrives on
 };
 
 template <int L>
@@ -64,11 +65,13 @@ __global__ void __launch_bounds__(Geo<L>::THREADS, 1) k_mx_fft2(MxFft2Args a) {
     unsigned char *b2 = smem + G::FN2_BYTES;                 // stage-2 operand, then the output staging
     float *red = reinterpret_cast<float *>(b2 + G::B2_BYTES);
     __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t unarmed;                 // test hook: nothing ever arrives here
     __shared__ uint32_t tbase;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, q = warp & 3, g = warp >> 2;
     if (warp == 0) tc::tmem_alloc(&tbase, G::TMEM_COLS);
     if (tid == 0) {
         tc::mbar_init(&bar, 1);
+        tc::mbar_init(&unarmed, 1);
         tc::mbar_fence_init();
     }
     F::load_fn2(a.fn2, fn2, tid);
@@ -151,6 +154,10 @@ __global__ void __launch_bounds__(Geo<L>::THREADS, 1) k_mx_fft2(MxFft2Args a) {
     if (r + step < a.rows) load_row(r + step);
     tc::fence_before_sync();
     __syncthreads();
+    if (a.probe > 0) {                                        // the bounded-wait path, before any MMA
+        const bool mine = tc::mbar_wait(&unarmed, 0, (uint32_t)a.probe);
+        ok = __syncthreads_and(mine) != 0;
+    }
     if (tid == 0 && ok) {
         tc::fence_after_sync();
         F::issue_stage1(tm, fn2_s);
@@ -438,7 +445,7 @@ size_t pass2_smem(int m) {
 template <int L>
 cudaError_t launch_mx_fft2(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st) {
     MxFft2Args p{d.y1, d.twn, d.mx_fn2n, d.mx_f128, out, d.mx_err, d.n, d.npad, d.m2,
-                 d.layout == PFA_LAYOUT_CENTRED, detect, d.sgn > 0, scale};
+                 d.layout == PFA_LAYOUT_CENTRED, detect, d.sgn > 0, scale, d.mx_probe};
     const size_t sm = fft2_smem<L>();
     auto fn = k_mx_fft2<L>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

@@ -33,7 +33,7 @@ class Config(C.Structure):
     _fields_ = [("mode", C.c_int32), ("m", C.c_int32), ("n", C.c_int32), ("grid", C.c_int32),
                 ("range_interp", C.c_int32), ("az_interp", C.c_int32), ("device", C.c_int32),
                 ("fft_ept_cross", C.c_int32), ("fft_ept_range", C.c_int32), ("detect_order", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("test_wait_polls", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class FixedJob(C.Structure):

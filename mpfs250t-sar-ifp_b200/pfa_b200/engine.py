@@ -191,13 +191,15 @@ class FloatPlan(_Plan):
     DETECT = {"mag": _lib.DETECT_MAG, "power": _lib.DETECT_POWER, "complex": _lib.DETECT_COMPLEX}
 
     def __init__(self, m: int, n: int, range_sinc: bool = False, az_sinc: bool = False, mixed: bool = False,
-                 device: int = 0, tile: tuple = (0, 0)):
+                 device: int = 0, tile: tuple = (0, 0), test_wait_polls: int = 0):
         """``tile``: complex values per thread of the (cross, range) FFTs, 8, 16 or 32, 0 = the library's
-        automatic choice (the autotuner's knob)."""
+        automatic choice (the autotuner's knob).  ``test_wait_polls``: the test hook of pfa_config (0 in
+        normal use)."""
         cfg = _lib.Config(mode=_lib.MODE_MIXED if mixed else _lib.MODE_FLOAT32, m=m, n=n, grid=0,
                           range_interp=_lib.SINC if range_sinc else _lib.LERP,
                           az_interp=_lib.SINC if az_sinc else _lib.LERP, device=device,
-                          fft_ept_cross=int(tile[0]), fft_ept_range=int(tile[1]))
+                          fft_ept_cross=int(tile[0]), fft_ept_range=int(tile[1]),
+                          test_wait_polls=int(test_wait_polls))
         super().__init__(cfg)
         self.m, self.n, self.device, self.tile = m, n, device, tuple(tile)
         self.m2, self.n2 = geometry.pow2(m), geometry.pow2(n)

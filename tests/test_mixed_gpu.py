@@ -84,3 +84,22 @@ def test_mixed_full_size_vs_fp32(torch_cuda):
         b = pmx.form(sig, detect="complex")
         err = float(torch.linalg.vector_norm(b - a) / torch.linalg.vector_norm(a))
     assert err <= TOL, err
+
+
+def test_bounded_wait_runs_out_and_the_context_recovers(torch_cuda):
+    """Every tensor-core completion wait is bounded.  A plan whose range FFT first waits on a barrier that
+    nothing arrives on (the test hook pfa_config.test_wait_polls) gives up, issues no MMA, and the
+    synchronous entry point returns PFA_ERR_TIMEOUT; the context stays usable and a normal plan right
+    after forms the correct frame."""
+    from pfa_b200 import _lib
+    sc = synth.make_scene(600, 2000, n_targets=8, clutter_db=-10.0, snr_db=20.0, seed=66)   # range: 2048 points
+    tb = geometry.prepare_tables_from_scene(sc)
+    with engine.FloatPlan(600, 2000, mixed=True, test_wait_polls=2000) as p:
+        p.set_tables(tb)
+        with pytest.raises(_lib.PfaError) as ei:
+            p.form_host(sc.signal)
+        assert ei.value.status == _lib.TIMEOUT
+        assert "timed out" in str(ei.value)
+    mx = _run(sc.signal, tb, True, detect="complex")
+    f32 = _run(sc.signal, tb, False, detect="complex")
+    assert fp.rel_l2(mx, f32) <= TOL
