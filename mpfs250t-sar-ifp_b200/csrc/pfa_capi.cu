@@ -91,16 +91,35 @@ struct DeviceGuard {
 
 namespace pfa {
 
+// Byte offsets of the fixed job vectors inside FixedDev::job_block (256-byte aligned each).
+struct FixedJobLayout {
+    size_t f0, df, fac, tan_s, order, krp, kcp, hamr, hamc, tw, sinc, total;
+    FixedJobLayout(int m, int G) {
+        size_t o = 0;
+        auto take = [&](size_t bytes) { const size_t at = o; o += (bytes + 255) / 256 * 256; return at; };
+        f0 = take(4u * m); df = take(4u * m); fac = take(4u * m); tan_s = take(4u * m); order = take(4u * m);
+        krp = take(4u * G); kcp = take(4u * G); hamr = take(4u * G); hamc = take(4u * G); tw = take(4u * G);
+        sinc = take(2u * 256 * 32);
+        total = o;
+    }
+};
+
 cudaError_t fixed_alloc(FixedDev &d, int m, int n, int G) {
     size_t acc = 0;
     cudaError_t e = cudaSuccess;
     d.m = m; d.n = n; d.G = G; d.L = ilog2(G); d.mpad = (m + 31) / 32 * 32;
 #define TRY(x) do { e = (x); if (e != cudaSuccess) return e; } while (0)
-    TRY(dalloc(&d.f0, m, &acc)); TRY(dalloc(&d.df, m, &acc)); TRY(dalloc(&d.fac, m, &acc));
-    TRY(dalloc(&d.tan_s, m, &acc)); TRY(dalloc(&d.order, m, &acc));
-    TRY(dalloc(&d.krp, G, &acc)); TRY(dalloc(&d.kcp, G, &acc));
-    TRY(dalloc(&d.hamr, G, &acc)); TRY(dalloc(&d.hamc, G, &acc));
-    TRY(dalloc(&d.tw, G, &acc)); TRY(dalloc(&d.sinc, 256 * 32, &acc));
+    const FixedJobLayout lay(m, G);
+    TRY(cudaMalloc(&d.job_block, lay.total));
+    d.job_bytes = lay.total;
+    acc += lay.total;
+    unsigned char *jb = static_cast<unsigned char *>(d.job_block);
+    d.f0 = reinterpret_cast<float *>(jb + lay.f0); d.df = reinterpret_cast<float *>(jb + lay.df);
+    d.fac = reinterpret_cast<float *>(jb + lay.fac); d.tan_s = reinterpret_cast<float *>(jb + lay.tan_s);
+    d.order = reinterpret_cast<int32_t *>(jb + lay.order);
+    d.krp = reinterpret_cast<float *>(jb + lay.krp); d.kcp = reinterpret_cast<float *>(jb + lay.kcp);
+    d.hamr = reinterpret_cast<int32_t *>(jb + lay.hamr); d.hamc = reinterpret_cast<int32_t *>(jb + lay.hamc);
+    d.tw = reinterpret_cast<uint32_t *>(jb + lay.tw); d.sinc = reinterpret_cast<int16_t *>(jb + lay.sinc);
     TRY(dalloc(&d.p1, (size_t)n * d.mpad, &acc));
     TRY(dalloc(&d.y1, (size_t)n * G, &acc));
     TRY(dalloc(&d.y2, (size_t)G * G, &acc));
@@ -111,9 +130,13 @@ cudaError_t fixed_alloc(FixedDev &d, int m, int n, int G) {
 }
 
 void fixed_free(FixedDev &d) {
-    dfree(d.f0); dfree(d.df); dfree(d.fac); dfree(d.tan_s); dfree(d.order); dfree(d.krp); dfree(d.kcp);
-    dfree(d.hamr); dfree(d.hamc); dfree(d.tw); dfree(d.sinc); dfree(d.p1); dfree(d.y1); dfree(d.y2);
-    dfree(d.e1); dfree(d.e2); dfree(d.ctrl);
+    if (d.job_block) cudaFree(d.job_block);
+    d.job_block = nullptr;
+    d.f0 = d.df = d.fac = d.tan_s = d.krp = d.kcp = nullptr;
+    d.order = d.hamr = d.hamc = nullptr;
+    d.tw = nullptr;
+    d.sinc = nullptr;
+    dfree(d.p1); dfree(d.y1); dfree(d.y2); dfree(d.e1); dfree(d.e2); dfree(d.ctrl);
 }
 
 }  // namespace pfa
@@ -238,48 +261,74 @@ pfa_status pfa_set_fixed_job(pfa_plan *p, const pfa_fixed_job *job) {
     DeviceGuard dg(p->device);
     pfa::FixedDev &d = p->fx;
     const int m = d.m, G = d.G;
+    // The whole job goes up as one copy of its host image; the grid-dependent tables (twiddles, sinc) are
+    // re-derived only when their inputs differ from the previous job's.
+    const pfa::FixedJobLayout lay(m, G);
+    std::vector<unsigned char> &img = p->job_host;
+    const bool first = img.size() != lay.total;
+    if (first) img.assign(lay.total, 0);
+    auto at = [&](size_t off) { return img.data() + off; };
+    std::memcpy(at(lay.f0), job->f0, 4u * m);
+    std::memcpy(at(lay.df), job->df, 4u * m);
+    std::memcpy(at(lay.tan_s), job->tan_s, 4u * m);
     // pass-1 source scale f32(f32(2 pr) / f32(c)) (NumPy 2 float32 arithmetic, silicon_emulator.py:144)
-    std::vector<float> fac(m);
+    float *fac = reinterpret_cast<float *>(at(lay.fac));
     const float c32 = (float)299792458.0;
     for (int i = 0; i < m; ++i) {
         volatile float two_pr = 2.0f * job->pr[i];
         fac[i] = two_pr / c32;
     }
     // sorted slot -> pulse (inverse of inv_order); reject non-permutations
-    std::vector<int32_t> order(m, -1);
+    int32_t *order = reinterpret_cast<int32_t *>(at(lay.order));
+    for (int i = 0; i < m; ++i) order[i] = -1;
     for (int i = 0; i < m; ++i) {
         const int r = job->inv_order[i];
         if (r < 0 || r >= m || order[r] != -1) return fail(p, PFA_ERR_BAD_ARG, "inv_order is not a permutation");
         order[r] = i;
     }
-    std::vector<int32_t> hr(G), hc(G);
-    if (job->ham_r) std::memcpy(hr.data(), job->ham_r, sizeof(int32_t) * G); else pfa::build_hamming_q15(d.n, G, hr.data());
-    if (job->ham_c) std::memcpy(hc.data(), job->ham_c, sizeof(int32_t) * G); else pfa::build_hamming_q15(m, G, hc.data());
-    std::vector<int16_t> tw2(G);
-    if (job->twiddle) std::memcpy(tw2.data(), job->twiddle, sizeof(int16_t) * G); else pfa::build_twiddles_q15(G, tw2.data());
-    // stage-contiguous layout: stage s (span 2^s) entries k < 2^(s-1) at offset 2^(s-1)-1
-    std::vector<uint32_t> tws(G, 0u);
-    const int L = d.L;
-    for (int b = 0; b < L; ++b) {
-        for (int k = 0; k < (1 << b); ++k) {
-            const int src = k << (L - 1 - b);
-            tws[(1 << b) - 1 + k] = (uint32_t)(uint16_t)tw2[2 * src] | ((uint32_t)(uint16_t)tw2[2 * src + 1] << 16);
+    std::memcpy(at(lay.krp), job->kr_grid, 4u * G);
+    std::memcpy(at(lay.kcp), job->kc_grid, 4u * G);
+    int32_t *hr = reinterpret_cast<int32_t *>(at(lay.hamr));
+    int32_t *hc = reinterpret_cast<int32_t *>(at(lay.hamc));
+    if (job->ham_r) std::memcpy(hr, job->ham_r, 4u * G); else pfa::build_hamming_q15(d.n, G, hr);
+    if (job->ham_c) std::memcpy(hc, job->ham_c, 4u * G); else pfa::build_hamming_q15(m, G, hc);
+    // twiddles: stage-contiguous layout, stage s (span 2^s) entries k < 2^(s-1) at offset 2^(s-1)-1
+    const bool tw_same = !first && (job->twiddle ? (p->last_tw_builtin == 0 && p->last_tw_in.size() == (size_t)G &&
+                                                    std::memcmp(p->last_tw_in.data(), job->twiddle, 2u * G) == 0)
+                                                 : p->last_tw_builtin == 1);
+    if (!tw_same) {
+        std::vector<int16_t> tw2(G);
+        if (job->twiddle) std::memcpy(tw2.data(), job->twiddle, sizeof(int16_t) * G); else pfa::build_twiddles_q15(G, tw2.data());
+        uint32_t *tws = reinterpret_cast<uint32_t *>(at(lay.tw));
+        std::memset(tws, 0, 4u * G);
+        const int L = d.L;
+        for (int b = 0; b < L; ++b) {
+            for (int k = 0; k < (1 << b); ++k) {
+                const int src = k << (L - 1 - b);
+                tws[(1 << b) - 1 + k] = (uint32_t)(uint16_t)tw2[2 * src] | ((uint32_t)(uint16_t)tw2[2 * src + 1] << 16);
+            }
         }
+        p->last_tw_builtin = job->twiddle ? 0 : 1;
+        if (job->twiddle) p->last_tw_in.assign(job->twiddle, job->twiddle + G); else p->last_tw_in.clear();
     }
-    std::vector<int16_t> sinc_pt(256 * 32), sinc(256 * 32);
-    if (job->sinc_q15) std::memcpy(sinc_pt.data(), job->sinc_q15, sizeof(int16_t) * 256 * 32); else pfa::build_sinc_table(sinc_pt.data());
-    if (!pfa::sinc_table_fits_int32(sinc_pt.data()))
-        return fail(p, PFA_ERR_BAD_ARG, "sinc table: sum |tap| over a half of a phase exceeds 65535");
-    for (int ph = 0; ph < 256; ++ph)          // device layout [tap][phase]
-        for (int t = 0; t < 32; ++t) sinc[t * 256 + ph] = sinc_pt[ph * 32 + t];
-    cudaError_t e;
-#define CPY(dst, src, cnt) do { e = cudaMemcpy(dst, src, sizeof(*(dst)) * (cnt), cudaMemcpyHostToDevice); \
-        if (e != cudaSuccess) return cuda_fail(p, e, "job upload"); } while (0)
-    CPY(d.f0, job->f0, m); CPY(d.df, job->df, m); CPY(d.fac, fac.data(), m); CPY(d.tan_s, job->tan_s, m);
-    CPY(d.order, order.data(), m); CPY(d.krp, job->kr_grid, G); CPY(d.kcp, job->kc_grid, G);
-    CPY(d.hamr, hr.data(), G); CPY(d.hamc, hc.data(), G); CPY(d.tw, tws.data(), G);
-    CPY(d.sinc, sinc.data(), 256 * 32);
-#undef CPY
+    const bool sinc_same = !first && (job->sinc_q15 ? (p->last_sinc_builtin == 0 &&
+                                                       std::memcmp(p->last_sinc_in.data(), job->sinc_q15, 2u * 256 * 32) == 0)
+                                                    : p->last_sinc_builtin == 1);
+    if (!sinc_same) {
+        std::vector<int16_t> sinc_pt(256 * 32);
+        if (job->sinc_q15) std::memcpy(sinc_pt.data(), job->sinc_q15, sizeof(int16_t) * 256 * 32); else pfa::build_sinc_table(sinc_pt.data());
+        if (!pfa::sinc_table_fits_int32(sinc_pt.data())) {
+            p->last_sinc_builtin = -1;
+            return fail(p, PFA_ERR_BAD_ARG, "sinc table: sum |tap| over a half of a phase exceeds 65535");
+        }
+        int16_t *sinc = reinterpret_cast<int16_t *>(at(lay.sinc));
+        for (int ph = 0; ph < 256; ++ph)          // device layout [tap][phase]
+            for (int t = 0; t < 32; ++t) sinc[t * 256 + ph] = sinc_pt[ph * 32 + t];
+        p->last_sinc_builtin = job->sinc_q15 ? 0 : 1;
+        if (job->sinc_q15) p->last_sinc_in.assign(job->sinc_q15, job->sinc_q15 + 256 * 32); else p->last_sinc_in.clear();
+    }
+    const cudaError_t e = cudaMemcpy(d.job_block, img.data(), lay.total, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(p, e, "job upload");
     p->job_ready = true;
     return PFA_OK;
 }

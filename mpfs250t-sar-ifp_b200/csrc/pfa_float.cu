@@ -1021,20 +1021,23 @@ pfa_status pfa_set_float_job(pfa_plan *p, const pfa_float_job *job) {
     d.sgn = job->sgn < 0 ? -1 : 1;
     d.layout = job->layout;
     d.window = (job->ham_m && job->ham_n) ? 1 : 0;
-    std::vector<float2> twm, twn;
-    pfa::full_twiddles(d.m2, twm);
-    pfa::full_twiddles(d.n2, twn);
-    std::vector<int16_t> tabq(pfa::kTabShorts, 0);
-    const int16_t *tq = pfa::builtin_sinc_table();
-    for (int i = 0; i < 256 * 32; ++i) tabq[(i >> 5) * pfa::kTabRow + (i & 31)] = tq[i];   // [phase][tap], padded rows
     cudaError_t e;
 #define CPY(dst, src, cnt) do { e = cudaMemcpy(dst, src, sizeof(*(dst)) * (cnt), cudaMemcpyHostToDevice); \
         if (e != cudaSuccess) return fcuda(p, e, "float job upload"); } while (0)
+    if (!d.consts_ready) {      // twiddles and the sinc table depend on the plan's shape only
+        std::vector<float2> twm, twn;
+        pfa::full_twiddles(d.m2, twm);
+        pfa::full_twiddles(d.n2, twn);
+        std::vector<int16_t> tabq(pfa::kTabShorts, 0);
+        const int16_t *tq = pfa::builtin_sinc_table();
+        for (int i = 0; i < 256 * 32; ++i) tabq[(i >> 5) * pfa::kTabRow + (i & 31)] = tq[i];   // [phase][tap], padded rows
+        CPY(d.twm, twm.data(), d.m2); CPY(d.twn, twn.data(), d.n2);
+        CPY(d.tabq, tabq.data(), pfa::kTabShorts);
+        d.consts_ready = true;
+    }
     CPY(d.f0, job->f0, m); CPY(d.df, job->df, m); CPY(d.flast, job->f_last, m); CPY(d.pr, job->pr, m); CPY(d.tan_s, job->tan_s, m);
     CPY(d.order, job->order, m); CPY(d.kr, job->kr_grid, n); CPY(d.kc, job->kc_grid, m);
     if (d.window) { CPY(d.ham_m64, job->ham_m, m); CPY(d.ham_n64, job->ham_n, n); }
-    CPY(d.twm, twm.data(), d.m2); CPY(d.twn, twn.data(), d.n2);
-    CPY(d.tabq, tabq.data(), pfa::kTabShorts);
 #undef CPY
     p->job_ready = true;
     return PFA_OK;

@@ -6,6 +6,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/pfa_b200.h"
 
@@ -31,6 +32,8 @@ struct FixedDev {
     int32_t *e1 = nullptr;             // [G]
     int32_t *e2 = nullptr;             // [G]
     int32_t *ctrl = nullptr;           // [0] q0 max bits, [1] emax1, [2] emax2, [3] q0 exponent
+    void *job_block = nullptr;         // the job vectors above (f0 .. sinc) in one allocation
+    size_t job_bytes = 0;
 };
 
 struct FloatDev {
@@ -42,6 +45,7 @@ struct FloatDev {
     int32_t *order = nullptr;
     float2 *twm = nullptr, *twn = nullptr;      // stage-contiguous twiddles for m2 and n2
     int16_t *tabq = nullptr;                    // sinc table (Q15 taps), [phase][tap] rows of 40 int16
+    bool consts_ready = false;                  // twm, twn and tabq (plan constants) uploaded
     int window = 1;
     float2 *p1 = nullptr;              // [n][mpad] pass-1 output (range-bin rows, sorted pulses)
     float2 *y1 = nullptr;              // [m2][npad] cross FFT output, transposed (cross-bin rows)
@@ -95,6 +99,11 @@ struct pfa_plan {
     void *pipe_in[2] = {nullptr, nullptr}, *pipe_out[2] = {nullptr, nullptr};
     size_t pipe_in_bytes = 0, pipe_out_bytes = 0;
     cudaEvent_t pipe_ev[6] = {};      // uploaded[2], computed[2], downloaded[2]
+    // fixed job staging: the host image of FixedDev::job_block (one upload per job) and the inputs the
+    // grid-dependent tables were last derived from (rebuilt only when those change)
+    std::vector<unsigned char> job_host;
+    std::vector<int16_t> last_tw_in, last_sinc_in;
+    int last_tw_builtin = -1, last_sinc_builtin = -1;
     pfa::StageProf prof;
     std::string err;
 };

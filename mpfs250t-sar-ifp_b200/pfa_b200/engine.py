@@ -114,8 +114,11 @@ class FixedPlan(_Plan):
 
     def set_tables(self, tables: dict):
         """Upload the job derived from ``prepare_tables`` output (mpfs/host/sar_pipeline.py:36-115)."""
-        job = geometry.fixed_job(tables, self.grid)
-        return self.set_job(job)
+        return self.set_job(self.job_for(tables))
+
+    def job_for(self, tables: dict) -> dict:
+        """The job of ``tables`` (host only, no device work: safe on another host thread)."""
+        return geometry.fixed_job(tables, self.grid)
 
     def set_job(self, job: dict):
         inv_order = np.empty(job["m"], np.int32)
@@ -206,7 +209,13 @@ class FloatPlan(_Plan):
 
     def set_tables(self, tables: dict, window: bool = True, centred: bool = True):
         """Upload the job derived from ``prepare_tables`` output (mpfs/host/sar_pipeline.py:36-115)."""
-        job = geometry.float_job(tables)
+        return self.set_job(self.job_for(tables), window, centred)
+
+    def job_for(self, tables: dict) -> dict:
+        """The job of ``tables`` (host only, no device work: safe on another host thread)."""
+        return geometry.float_job(tables)
+
+    def set_job(self, job: dict, window: bool = True, centred: bool = True):
         keep = dict(f0=job["f0"], df=job["df"], fl=job["f_last"], pr=job["pr"], tan_s=job["tan_s"],
                     order=job["order"], kr=job["KR"], kc=job["KC"], hm=np.ascontiguousarray(job["ham_m"]),
                     hn=np.ascontiguousarray(job["ham_n"]))
@@ -251,6 +260,35 @@ class FloatPlan(_Plan):
         _lib.check(self._lib.pfa_form_float_host_frames(self._h, _frame_ptrs(sigs), _frame_ptrs(imgs),
                                                         self.DETECT[detect], len(sigs)), self._h)
         return imgs
+
+def form_host_scenes(plan, scenes, prepare, outs=None, **form_kw):
+    """A queue of scenes with a new geometry each, through the host-buffer entry point (the reference's
+    scene loop, mpfs/host/sar_pipeline.py:151-163).
+
+    ``prepare(scene) -> (tables, signal)`` (CPHD read, ``prepare_tables``) and the job derivation of scene
+    i + 1 run on a host thread while scene i is formed: the library call releases the interpreter lock,
+    so table preparation leaves the critical path and each scene costs its frame plus the one-copy job
+    upload.  ``outs``: output arrays reused in turn (the caller consumes each image before its buffer
+    comes round again); default a new array per scene.  Returns the images in scene order."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    def stage(sc):
+        tables, signal = prepare(sc)
+        return plan.job_for(tables), signal
+
+    scenes = list(scenes)
+    images = []
+    with ThreadPoolExecutor(max_workers=1, thread_name_prefix="pfa-scene-prep") as ex:
+        nxt = ex.submit(stage, scenes[0]) if scenes else None
+        for i in range(len(scenes)):
+            job, signal = nxt.result()
+            if i + 1 < len(scenes):
+                nxt = ex.submit(stage, scenes[i + 1])
+            plan.set_job(job)
+            out = outs[i % len(outs)] if outs else None
+            images.append(plan.form_host(signal, out, **form_kw))
+    return images
+
 
 def focus_float(signal, tables, range_sinc=False, az_sinc=False, mixed=False, device=0):
     """Drop-in for ``accel.NumpyBackend.focus`` (mpfs/host/accel.py:39-44): float32 |img|."""

@@ -16,6 +16,7 @@ frequency row is affine in the sample index, so its extreme wavenumbers are its 
 """
 from __future__ import annotations
 
+import functools
 import math
 
 import numpy as np
@@ -173,19 +174,26 @@ def pow2(v: int) -> int:
     return 1 << int(math.ceil(math.log2(max(int(v), 1))))
 
 
+@functools.lru_cache(maxsize=64)
 def hamming_q15_floor(length: int, size: int) -> np.ndarray:
-    """floor(hamming(length) * 32768) zero-padded to ``size`` (int32; the odd-length centre is 32768)."""
+    """floor(hamming(length) * 32768) zero-padded to ``size`` (int32; the odd-length centre is 32768).
+    Cached per (length, size): a queue of same-shaped scenes builds it once (read-only array)."""
     h = np.zeros(size)
     h[:length] = np.hamming(length)
-    return np.floor(h * 32768).astype(np.int32)
+    out = np.floor(h * 32768).astype(np.int32)
+    out.flags.writeable = False
+    return out
 
 
+@functools.lru_cache(maxsize=16)
 def twiddles_q15(n: int) -> np.ndarray:
-    """(n/2, 2) int16: floor(exp(-2 pi j k/n) * 32768) clipped to int16 (src/fixedpoint.py:277)."""
+    """(n/2, 2) int16: floor(exp(-2 pi j k/n) * 32768) clipped to int16 (src/fixedpoint.py:277).
+    Cached per n (read-only array)."""
     w = np.exp(-2j * np.pi * np.arange(n // 2) / n)
     out = np.empty((n // 2, 2), np.int16)
     out[:, 0] = np.clip(np.floor(w.real / 2.0 ** -15), -32768, 32767)
     out[:, 1] = np.clip(np.floor(w.imag / 2.0 ** -15), -32768, 32767)
+    out.flags.writeable = False
     return out
 
 
