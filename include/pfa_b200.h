@@ -87,10 +87,11 @@ typedef struct pfa_config {
     int32_t fft_ept_range; /* float: same for the range FFT (pow2(n)/ept threads; 0 = automatic:
                               32 for lines of 8192 and 16384 points, else 16)                    */
     int32_t detect_order;  /* fixed: pfa_detect_order (0 = emulator order)                      */
-    int32_t test_wait_polls; /* test hook, 0 in normal use.  > 0 (mixed mode): the tensor-core range
-                              FFT first waits this many polls on a barrier nothing arrives on, so
-                              its bounded-wait path runs: no MMA is issued, the frame is zeros and
-                              the synchronous entry points return PFA_ERR_TIMEOUT                 */
+    int32_t test_wait_polls; /* test hook, 0 in normal use.  > 0: a bounded wait first waits this many
+                              polls on a barrier nothing arrives on, so its timeout path runs --
+                              FP32 mode: the cross pass's TMA row load (rows are not used); mixed
+                              mode: the tensor-core range FFT (no MMA is issued).  The frame is
+                              zeros and the synchronous entry points return PFA_ERR_TIMEOUT      */
     int32_t reserved[5];
 } pfa_config;
 

@@ -208,11 +208,11 @@ pfa_status pfa_plan_create(const pfa_config *cfg, pfa_plan **out) {
         }
         p->fl.ept_cross = c.fft_ept_cross;      // 0: the automatic choice of the dispatch
         p->fl.ept_range = c.fft_ept_range;
+        p->fl.mx_probe = c.test_wait_polls > 0 ? c.test_wait_polls : 0;
         p->ws_bytes = pfa::float_workspace_bytes(c.m, c.n);
         if (e == cudaErrorInvalidValue) { pfa::float_free(p->fl); delete p; return PFA_ERR_BAD_CONFIG; }
         if (e == cudaSuccess && c.mode == PFA_MODE_MIXED) {
             p->fl.mixed = 1;
-            p->fl.mx_probe = c.test_wait_polls > 0 ? c.test_wait_polls : 0;
             e = pfa::mixed_prepare(p->fl);
         }
     } else {

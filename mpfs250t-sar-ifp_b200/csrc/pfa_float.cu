@@ -22,6 +22,8 @@
 #include "fft_f32.cuh"
 #include "interp_f32.cuh"
 #include "pfa_internal.h"
+#include "tc_sm100.cuh"
+#include "tma_sm100.cuh"
 
 namespace pfa {
 const int16_t *builtin_sinc_table();
@@ -245,14 +247,26 @@ __device__ __forceinline__ int br_low(uint32_t p) { return (int)((p >> 17) & 0x3
 
 // ------------------------------------------------------------------------------------------ K2f
 struct FPass2Args {
-    const float2 *p1;
+    CUtensorMap p1_map;   // TMA map of the pass-1 output rows (boxes of 256 samples)
     const double *tan_s, *kr_grid, *kc_grid, *ham_m, *ham_n;
     const int16_t *tabq;
     const float2 *tw;
     float2 *y1t;          // [m2][npad] cross-FFT output, transposed: row = cross bin, col = range bin
     uint32_t *pk_out;     // lerp: packed brackets [j][k] for the autofocus adjoint, or nullptr
+    int *err;             // set when the row load's bounded wait runs out
     int m, n, mpad, npad, centred, window, inverse;
+    int probe;            // test hook: > 0 = first wait this many polls on a barrier nothing arrives on
 };
+
+// Polls of the pass-2 row-load wait (each try_wait may suspend for a while): a TMA row load lands in
+// microseconds, so running out means the copy is lost; the frame is then flagged, not waited for.
+constexpr uint32_t kRowWaitPolls = 1u << 22;
+
+// Shared-memory bytes of pass 2's region A: the row as whole 256-sample boxes, or the FFT exchange buffer.
+__host__ __device__ constexpr size_t pass2_region_a(int m, size_t xbuf_elems) {
+    return ((size_t)2048 * ((m + 255) / 256) > (size_t)8 * xbuf_elems ? (size_t)2048 * ((m + 255) / 256)
+                                                                       : (size_t)8 * xbuf_elems);
+}
 
 // Corner turn #2 fused into the cross FFT: a cluster of kCT CTAs holds kCT adjacent range bins; after
 // their FFTs each CTA writes a 1/kCT slice of cross bins for all kCT rows (kCT * 8-byte runs) into the
@@ -266,30 +280,41 @@ static_assert(8 % kCT == 0, "npad (a multiple of 8) must hold whole clusters");
 // that the frame's pass 2 carries no extra register pressure)
 template <int L, int E, bool SINC, bool PK = false>
 __global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, fl_min_ctas(L, E))
-k_fl_pass2_fft(FPass2Args a) {
+k_fl_pass2_fft(const __grid_constant__ FPass2Args a) {
     using F = F32Fft<L, E>;
     constexpr int N = F::N, T = F::T;
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(1024) unsigned char smem[];
+    // layout: [region A: the row (whole TMA boxes) | exchange buffer] [sinc table] [row mbarrier, probe]
     const int m = a.m;
-    const size_t regA = (max((size_t)8 * m, (size_t)8 * F::xbuf_elems()) + 15) & ~(size_t)15;
+    const size_t regA = pass2_region_a(m, F::xbuf_elems());
     float2 *row = reinterpret_cast<float2 *>(smem);
     float2 *xbuf = reinterpret_cast<float2 *>(smem);
     int16_t *tab = reinterpret_cast<int16_t *>(smem + regA);
+    uint64_t *row_bar = reinterpret_cast<uint64_t *>(smem + regA + (SINC ? 2 * kTabShorts : 0));
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     const int tid = threadIdx.x;
     const int j = blockIdx.x;
     const bool live = j < a.n;                 // grid is padded to a multiple of the cluster size
     float2 x[E];
+    bool landed = true, issued = false;
     if (live) {
-    // the row (and the sinc table) stream into shared memory while the brackets are computed
-    {
-        const float2 *src = a.p1 + (size_t)j * a.mpad;      // 256-byte aligned rows
-        const int nchunk = (m + 1) >> 1;                      // 16-byte chunks (the pad covers odd m)
-        for (int c = tid; c < nchunk; c += T) cp_async16(row + 2 * c, src + 2 * c);
-        if (SINC)
-            for (int c = tid; c < kTabShorts / 8; c += T) cp_async16(tab + 8 * c, a.tabq + 8 * c);
-        cp_async_commit();
+    // The row (256-sample boxes of the p1 tensor map) and the sinc table stream into shared memory by TMA
+    // while the brackets are computed; warp 0 issues the copies.
+    issued = (tma::saddr(row) & 127) == 0;          // CTA-uniform; a misaligned box is never issued
+    if (tid == 0) {
+        tc::mbar_init(row_bar, 1);
+        tc::mbar_init(row_bar + 1, 1);     // the test hook's barrier: never arrived on
+        tc::mbar_fence_init();
+        tc::fence_smem_to_async();
+    }
+    __syncthreads();
+    if (tid < 32 && issued) {
+        const int nbox = (m + 255) >> 8;
+        if (tid == 0) tma::arrive_expect_tx(row_bar, 2048u * nbox + (SINC ? 2u * kTabShorts : 0u));
+        __syncwarp();
+        for (int b = tid; b < nbox; b += 32) tma::load_2d(row + 256 * b, &a.p1_map, 256 * b, j, row_bar);
+        if (SINC && tid == 0) tma::bulk_load(tab, a.tabq, 2u * kTabShorts, row_bar);
     }
     const double krj = a.kr_grid[j];
     const double s0 = krj * a.tan_s[0], s1 = krj * a.tan_s[m - 1];
@@ -337,13 +362,23 @@ k_fl_pass2_fft(FPass2Args a) {
             }
         }
     }
-    cp_async_wait_all();
-    __syncthreads();
+    // sinc: warp 0 waits for the row and the block barrier passes its view of the landed bytes to the other
+    // warps; lerp: every thread waits (each measured the faster of the two for its kernel, by ~1 %)
+    const bool probe_ok = a.probe <= 0 || tc::mbar_wait(row_bar + 1, 0, (uint32_t)a.probe);
+    if constexpr (SINC) {
+        bool got = true;
+        if (tid < 32) got = issued && probe_ok && tc::mbar_wait(row_bar, 0, kRowWaitPolls);
+        landed = __syncthreads_and(got) != 0;
+    } else {
+        landed = issued && probe_ok && tc::mbar_wait(row_bar, 0, kRowWaitPolls);
+        __syncthreads();
+    }
+    if (!landed) atomicExch(a.err, 1);      // any thread whose wait ran out: the frame is not valid
 #pragma unroll
     for (int u = 0; u < E; ++u) {
         const int k = tid + T * u;
         float2 val = make_float2(0.f, 0.f);
-        if (k < m) {
+        if (k < m && landed) {
             if (bl[u] >= 0) {
                 const int lowi = bl[u] & 0xffff;
                 const Frac fr{bf[u], (bl[u] >> 16) & 0xff, (bl[u] >> 24) & 1};
@@ -379,6 +414,7 @@ k_fl_pass2_fft(FPass2Args a) {
         a.y1t[(size_t)k * a.npad + j0 + r] = remote[k];
     }
     cluster.sync();                            // keep this CTA's shared memory alive for the readers
+    if (issued && !landed) (void)tc::mbar_wait(row_bar, 0, kRowWaitPolls);   // no copy left in flight at exit
 }
 
 // ------------------------------------------------------------------------------------------ K3f
@@ -723,10 +759,10 @@ struct Cfg {
 template <int L, int E, bool SINC>
 cudaError_t launch_pass2(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, E>;
-    FPass2Args p{d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabq,
-                 d.twm, d.y1, d.pk_out, d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0};
-    size_t regA = (std::max((size_t)8 * d.m, (size_t)8 * F::xbuf_elems()) + 15) & ~(size_t)15;
-    size_t sm = regA + (SINC ? kTabShorts * 2 : 0);
+    FPass2Args p{d.p1_map, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabq, d.twm, d.y1, d.pk_out, d.wait_err,
+                 d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0,
+                 d.mixed ? 0 : d.mx_probe};
+    const size_t sm = pass2_region_a(d.m, F::xbuf_elems()) + (SINC ? kTabShorts * 2 : 0) + 16;   // + 2 mbarriers
     auto fn = k_fl_pass2_fft<L, E, SINC>;
     if (d.pk_out) fn = k_fl_pass2_fft<L, E, SINC, true>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -844,13 +880,16 @@ cudaError_t float_alloc(FloatDev &d, int m, int n) {
     TRY(dal(&d.twm, d.m2)); TRY(dal(&d.twn, d.n2));
     TRY(dal(&d.tabq, kTabShorts));
     TRY(dal(&d.p1, (size_t)n * d.mpad)); TRY(dal(&d.y1, (size_t)d.npad * d.m2));
+    TRY(dal(&d.wait_err, 1)); TRY(cudaMemset(d.wait_err, 0, sizeof(int)));
+    // pass 2 reads its range-bin row of p1 as 256-sample boxes (2 KB; the last one zero-filled past mpad)
+    TRY(tma::encode_2d(&d.p1_map, d.p1, 8, (uint64_t)d.mpad, (uint64_t)n, (uint64_t)8 * d.mpad, 256, 1));
 #undef TRY
     return cudaSuccess;
 }
 
 void float_free(FloatDev &d) {
     dfr(d.f0); dfr(d.df); dfr(d.flast); dfr(d.pr); dfr(d.tan_s); dfr(d.order); dfr(d.kr); dfr(d.kc); dfr(d.ham_m64);
-    dfr(d.ham_n64); dfr(d.twm); dfr(d.twn); dfr(d.tabq); dfr(d.p1); dfr(d.y1);
+    dfr(d.ham_n64); dfr(d.twm); dfr(d.twn); dfr(d.tabq); dfr(d.p1); dfr(d.y1); dfr(d.wait_err);
     dfr(d.af_zadj); dfr(d.af_acc); dfr(d.af_dacc); dfr(d.af_pk);
     mixed_free(d);
 }
@@ -1058,7 +1097,7 @@ pfa_status pfa_form_float(pfa_plan *p, const float *sig_dev, void *out_dev, int3
     return PFA_OK;
 }
 
-static pfa_status mixed_timeout_check(pfa_plan *p);
+static pfa_status wait_timeout_check(pfa_plan *p);
 
 pfa_status pfa_form_float_host(pfa_plan *p, const float *sig_host, void *out_host, int32_t detect) {
     if (!p || !sig_host || !out_host) return PFA_ERR_BAD_ARG;
@@ -1088,19 +1127,19 @@ pfa_status pfa_form_float_host(pfa_plan *p, const float *sig_host, void *out_hos
     if ((e = cudaMemcpyAsync(out_host, p->staging_out, out_b, cudaMemcpyDeviceToHost, p->host_stream)) != cudaSuccess)
         return fcuda(p, e, "d2h");
     if ((e = cudaStreamSynchronize(p->host_stream)) != cudaSuccess) return fcuda(p, e, "sync");
-    return mixed_timeout_check(p);
+    return wait_timeout_check(p);
 }
 
-// Mixed mode: a tensor-core completion wait that ran out sets a device flag; synchronous entry points read
-// (and clear) it after their frames and report PFA_ERR_TIMEOUT.
-static pfa_status mixed_timeout_check(pfa_plan *p) {
-    if (!p->fl.mixed || !p->fl.mx_err) return PFA_OK;
+// A bounded wait that ran out (pass 2's TMA row load; in mixed mode also a tensor-core completion) sets a
+// device flag; synchronous entry points read (and clear) it after their frames and report PFA_ERR_TIMEOUT.
+static pfa_status wait_timeout_check(pfa_plan *p) {
+    if (!p->fl.wait_err) return PFA_OK;
     int flag = 0;
-    cudaError_t e = cudaMemcpy(&flag, p->fl.mx_err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpy(&flag, p->fl.wait_err, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return fcuda(p, e, "timeout flag");
     if (!flag) return PFA_OK;
-    cudaMemset(p->fl.mx_err, 0, sizeof(int));
-    return ffail(p, PFA_ERR_TIMEOUT, "mixed mode: a tensor-core completion wait timed out (frame not valid)");
+    cudaMemset(p->fl.wait_err, 0, sizeof(int));
+    return ffail(p, PFA_ERR_TIMEOUT, "a bounded wait on the device timed out (frame not valid)");
 }
 
 static pfa_status float_frame(pfa_plan *p, const void *in, void *out, cudaStream_t st, int32_t detect) {
@@ -1117,7 +1156,7 @@ pfa_status pfa_form_float_host_frames(pfa_plan *p, const float *const *sig_hosts
     const size_t out_b = (detect == PFA_DETECT_COMPLEX ? 8 : 4) * (size_t)p->fl.m2 * p->fl.n2;
     const pfa_status st = pfa::run_host_frames(p, reinterpret_cast<const void *const *>(sig_hosts), out_hosts, nframes,
                                                in_b, out_b, float_frame, detect);
-    return st != PFA_OK ? st : mixed_timeout_check(p);
+    return st != PFA_OK ? st : wait_timeout_check(p);
 }
 
 pfa_status pfa_form_float_phase(pfa_plan *p, const float *sig_dev, const float *theta_dev, void *out_dev, int32_t detect,

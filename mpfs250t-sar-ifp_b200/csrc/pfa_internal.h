@@ -1,6 +1,7 @@
 // Internal plan state shared by the C-ABI glue and the kernel launchers.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -48,6 +49,7 @@ struct FloatDev {
     bool consts_ready = false;                  // twm, twn and tabq (plan constants) uploaded
     int window = 1;
     float2 *p1 = nullptr;              // [n][mpad] pass-1 output (range-bin rows, sorted pulses)
+    CUtensorMap p1_map;                // TMA map of p1: 8-byte elements, boxes of 256 x 1
     float2 *y1 = nullptr;              // [m2][npad] cross FFT output, transposed (cross-bin rows)
     int ept_cross = 0, ept_range = 0;    // FFT register tile (complex values per thread; 0 = automatic)
     float2 *af_zadj = nullptr;         // [n][m2] autofocus: adjoint of the range FFT (range-bin rows)
@@ -59,9 +61,10 @@ struct FloatDev {
     int mixed = 0;
     uint4 *mx_f128 = nullptr;          // F_128 TMEM image [128 lanes][256 columns] of fp16 pairs
     uint4 *mx_fn2m = nullptr, *mx_fn2n = nullptr;   // F_{m2/128}, F_{n2/128} shared-memory images
-    int *mx_err = nullptr;             // device flag: a tensor-core completion wait timed out
+    int *wait_err = nullptr;           // device flag: a bounded wait ran out (TMA row load, tensor-core completion)
     int mx_clusters = 0;               // resident 4-CTA clusters of the mixed pass 2
-    int mx_probe = 0;                  // test hook: polls of the range FFT's wait on an unarmed barrier
+    int mx_probe = 0;                  // test hook: polls of a wait on an unarmed barrier (FP32: pass 2's
+                                       // row load; mixed: the tensor-core range FFT)
     int sms = 0;                       // SM count of the plan's device
 };
 

@@ -10,7 +10,7 @@
 //
 // Both hold 512 TMEM columns, so they request enough shared memory that no two CTAs share an SM (a
 // second CTA would block in tcgen05.alloc; in a cluster that could deadlock with its own peer).  Every
-// completion wait is bounded; a timeout sets mx_err and the kernel finishes the line loop without
+// completion wait is bounded; a timeout sets wait_err and the kernel finishes the line loop without
 // issuing further MMAs (cluster barriers stay matched) and releases its TMEM.
 #include <cooperative_groups.h>
 #include <cuda_fp16.h>
@@ -444,7 +444,7 @@ size_t pass2_smem(int m) {
 
 template <int L>
 cudaError_t launch_mx_fft2(const FloatDev &d, void *out, int detect, float scale, cudaStream_t st) {
-    MxFft2Args p{d.y1, d.twn, d.mx_fn2n, d.mx_f128, out, d.mx_err, d.n, d.npad, d.m2,
+    MxFft2Args p{d.y1, d.twn, d.mx_fn2n, d.mx_f128, out, d.wait_err, d.n, d.npad, d.m2,
                  d.layout == PFA_LAYOUT_CENTRED, detect, d.sgn > 0, scale, d.mx_probe};
     const size_t sm = fft2_smem<L>();
     auto fn = k_mx_fft2<L>;
@@ -458,7 +458,7 @@ template <int L, bool SINC>
 cudaError_t launch_mx_pass2(const FloatDev &d, cudaStream_t st) {
     const int ngroups = d.npad / kMxCT;
     MxPass2Args p{d.p1, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabq, d.twm, d.mx_fn2m, d.mx_f128, d.y1,
-                  d.mx_err, d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0, ngroups};
+                  d.wait_err, d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0, ngroups};
     const size_t sm = pass2_smem<L, SINC>(d.m);
     auto fn = k_mx_pass2<L, SINC>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -558,18 +558,15 @@ cudaError_t mixed_prepare(FloatDev &d) {
         const std::vector<uint16_t> im = fn2_image(d.n2 / 128);
         if ((e = upload(&d.mx_fn2n, im.data(), im.size() * 2)) != cudaSuccess) return e;
     }
-    if ((e = cudaMalloc(&d.mx_err, sizeof(int))) != cudaSuccess) return e;
-    return cudaMemset(d.mx_err, 0, sizeof(int));
+    return cudaSuccess;
 }
 
 void mixed_free(FloatDev &d) {
     if (d.mx_f128) cudaFree(d.mx_f128);
     if (d.mx_fn2m) cudaFree(d.mx_fn2m);
     if (d.mx_fn2n) cudaFree(d.mx_fn2n);
-    if (d.mx_err) cudaFree(d.mx_err);
     d.mx_f128 = nullptr;
     d.mx_fn2m = d.mx_fn2n = nullptr;
-    d.mx_err = nullptr;
 }
 
 cudaError_t mixed_pass2(const FloatDev &d, cudaStream_t st) {

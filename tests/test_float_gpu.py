@@ -153,3 +153,35 @@ def test_16384_point_lines(torch_cuda, m, n, rs):
     cz = _run(sc.signal, tb, detect="complex", rs=rs, az=rs)
     assert cz.shape == (geometry.pow2(m), geometry.pow2(n))
     assert fp.rel_l2(cz, _f64_mixed(sc.signal, tb, rs, rs)) <= TOL
+
+
+@pytest.mark.parametrize("rs,az", [(False, False), (False, True)])
+@pytest.mark.parametrize("m", [255, 256, 257, 4099])
+def test_tma_row_boxes_cover_every_row_length(torch_cuda, m, rs, az):
+    """Pass 2 reads each range-bin row as 256-sample TMA boxes (the last one partly past the row, zero
+    filled): row lengths just below, at and above a box boundary and a long odd one match FP64."""
+    sc = synth.make_scene(m, 300, n_targets=12, clutter_db=-10.0, snr_db=20.0, seed=m, jitter=0.3)
+    tb = geometry.prepare_tables_from_scene(sc)
+    cz = _run(sc.signal, tb, detect="complex", rs=rs, az=az)
+    assert fp.rel_l2(cz, _f64_mixed(sc.signal, tb, rs, az)) <= TOL
+
+
+@pytest.mark.parametrize("az", [False, True])
+def test_row_load_bounded_wait_runs_out_and_the_context_recovers(torch_cuda, az):
+    """The TMA row load of pass 2 waits on an mbarrier with a poll limit.  A plan whose pass 2 first waits
+    on a barrier nothing arrives on (the test hook pfa_config.test_wait_polls) gives up, uses no row, waits
+    for its copies before it exits, and the synchronous entry point returns PFA_ERR_TIMEOUT; the context
+    stays usable and a normal plan right after forms the correct frame."""
+    sc = synth.make_scene(300, 260, n_targets=8, clutter_db=-10.0, snr_db=20.0, seed=67)
+    tb = geometry.prepare_tables_from_scene(sc)
+    with engine.FloatPlan(300, 260, False, az, test_wait_polls=500) as p:
+        p.set_tables(tb)
+        with pytest.raises(_lib.PfaError) as ei:
+            p.form_host(sc.signal)
+        assert ei.value.status == _lib.TIMEOUT
+        assert "timed out" in str(ei.value)
+        # the flag is cleared once reported: the next frame times out again rather than inheriting it
+        with pytest.raises(_lib.PfaError):
+            p.form_host(sc.signal)
+    cz = _run(sc.signal, tb, detect="complex", az=az)
+    assert fp.rel_l2(cz, _f64_mixed(sc.signal, tb, False, az)) <= TOL
