@@ -256,6 +256,7 @@ struct FPass2Args {
     int *err;             // set when the row load's bounded wait runs out
     int m, n, mpad, npad, centred, window, inverse;
     int probe;            // test hook: > 0 = first wait this many polls on a barrier nothing arrives on
+    double *ysum;         // PK (autofocus forward): += sum |y1|^2 over the frame (S / n2, by Parseval)
 };
 
 // Polls of the pass-2 row-load wait (each try_wait may suspend for a while): a TMA row load lands in
@@ -285,6 +286,7 @@ k_fl_pass2_fft(const __grid_constant__ FPass2Args a) {
     constexpr int N = F::N, T = F::T;
     extern __shared__ __align__(1024) unsigned char smem[];
     // layout: [region A: the row (whole TMA boxes) | exchange buffer] [sinc table] [row mbarrier, probe]
+    // [PK: T / 32 doubles of the |y1|^2 reduction].  No static shared memory: region A starts the window.
     const int m = a.m;
     const size_t regA = pass2_region_a(m, F::xbuf_elems());
     float2 *row = reinterpret_cast<float2 *>(smem);
@@ -393,6 +395,23 @@ k_fl_pass2_fft(const __grid_constant__ FPass2Args a) {
         x[u] = a.inverse ? make_float2(val.x, -val.y) : val;
     }
     F::run(x, xbuf, a.tw, tid);
+    if constexpr (PK) {
+        // the autofocus needs S = sum |z|^2 before its range adjoint: z = F_range y1 along zero-padded lines
+        // of n2, so S = n2 sum |y1|^2 (Parseval), summed here where y1 is formed
+        double *ysum_red = reinterpret_cast<double *>(row_bar + 2);   // dynamic: static shared memory
+        double sq = 0.0;                                              // would move region A off 128 bytes
+#pragma unroll
+        for (int v = 0; v < E; ++v) sq += (double)fmaf(x[v].x, x[v].x, x[v].y * x[v].y);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        if ((tid & 31) == 0) ysum_red[tid >> 5] = sq;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < T / 32; ++w) t += ysum_red[w];
+            atomicAdd(a.ysum, t);
+        }
+    }
     } else {
 #pragma unroll
         for (int v = 0; v < E; ++v) x[v] = make_float2(0.f, 0.f);
@@ -469,12 +488,16 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_fl_fft2(FFf
 //   g_p1 = R2^H (W . F_cross^H F_range^H g_z)
 //   dE/dtheta_i = 2 Im sum_j conj(g_p1[j, slot_i]) p1[j, slot_i]     (pass 1 is linear and per pulse,
 //                 so its adjoint never has to be formed)
-// The range FFT is recomputed from the cross-FFT buffer in the adjoint pass instead of storing z.
+// The range FFT is recomputed from the cross-FFT buffer in the adjoint pass instead of storing z.  One
+// pass over z suffices: S = n2 sum |y1|^2 comes from the forward pass 2 (Parseval), the range adjoint
+// takes the part -(1/S) log(I/S) z of g_z and sums I log I on the way, and the part -(E/S) z, whose
+// adjoint is -(E/S) n2 m2 R2^H (W^2 . R2 p1) (F^H F = N on the zero-padded lines), is added in the cross
+// adjoint, when E is known.
 struct AfRangeArgs {
     const float2 *y1t;      // [m2][npad] forward cross-FFT output, transposed
     const float2 *tw;       // range twiddles (n2)
-    double *acc;            // [0] sum I, [1] sum I log I
-    float2 *zadj_t;         // [n][m2] F_range^H g_z, range-bin rows
+    double *acc;            // [0] sum |y1|^2 (from the forward pass 2), [1] += sum I log I
+    float2 *zadj_t;         // [n][m2] F_range^H (-(1/S) log(I/S) z), range-bin rows
     int n, npad, m2;
 };
 
@@ -490,39 +513,6 @@ __device__ __forceinline__ void af_load_range_row(float2 (&x)[E], const AfRangeA
 }
 
 template <int L, int E>
-__global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_entropy(AfRangeArgs a) {
-    using F = F32Fft<L, E>;
-    constexpr int T = F::T;
-    extern __shared__ __align__(16) unsigned char smem[];
-    float2 *xbuf = reinterpret_cast<float2 *>(smem);
-    __shared__ double red[2][32];
-    const int tid = threadIdx.x;
-    float2 x[E];
-    af_load_range_row<L, E>(x, a, blockIdx.x);
-    F::run(x, xbuf, a.tw, tid);
-    double s = 0.0, h = 0.0;
-#pragma unroll
-    for (int v = 0; v < E; ++v) {
-        const float in = fmaf(x[v].x, x[v].x, x[v].y * x[v].y);
-        s += in;
-        if (in > 0.f) h += (double)in * (double)logf(in);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        s += __shfl_xor_sync(0xffffffffu, s, o);
-        h += __shfl_xor_sync(0xffffffffu, h, o);
-    }
-    if ((tid & 31) == 0) { red[0][tid >> 5] = s; red[1][tid >> 5] = h; }
-    __syncthreads();
-    if (tid == 0) {
-        double ss = 0.0, hh = 0.0;
-        for (int w = 0; w < T / 32; ++w) { ss += red[0][w]; hh += red[1][w]; }
-        atomicAdd(a.acc, ss);
-        atomicAdd(a.acc + 1, hh);
-    }
-}
-
-template <int L, int E>
 __global__ void __cluster_dims__(kCT, 1, 1) __launch_bounds__((1 << L) / E, fl_min_ctas(L, E))
 k_af_range_adjoint(AfRangeArgs a) {
     namespace cg = cooperative_groups;
@@ -533,19 +523,32 @@ k_af_range_adjoint(AfRangeArgs a) {
     cg::cluster_group cluster = cg::this_cluster();
     const int tid = threadIdx.x;
     const int k = blockIdx.x;                         // cross bin
-    const double S = a.acc[0];
-    const double Ent = log(S) - a.acc[1] / S;
-    const float invS = (float)(1.0 / S), off = (float)(Ent - log(S));
+    const double S = a.acc[0] * (double)N;
+    const float invS = (float)(1.0 / S), off = (float)(-log(S));
+    __shared__ double hred[T / 32];
     float2 x[E];
     af_load_range_row<L, E>(x, a, k);
     F::run(x, xbuf, a.tw, tid);                       // recompute z along range
+    float hf = 0.f;                                   // this thread's sum I log I (E values; double beyond)
 #pragma unroll
     for (int v = 0; v < E; ++v) {
         const float in = fmaf(x[v].x, x[v].x, x[v].y * x[v].y);
-        const float c = in > 0.f ? -invS * (logf(in) + off) : 0.f;     // dE/dI
-        x[v] = make_float2(c * x[v].x, -c * x[v].y);                    // conj(g_z)
+        const float lg = in > 0.f ? logf(in) : 0.f;
+        hf = fmaf(in, lg, hf);
+        const float c = in > 0.f ? -invS * (lg + off) : 0.f;            // -(1/S) log(I/S)
+        x[v] = make_float2(c * x[v].x, -c * x[v].y);                    // conj of that part of g_z
     }
+    double h = (double)hf;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+    if ((tid & 31) == 0) hred[tid >> 5] = h;
     F::run(x, xbuf, a.tw, tid);                       // F^H g = conj(F conj(g))
+    __syncthreads();                                  // hred complete
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < T / 32; ++w) t += hred[w];
+        atomicAdd(a.acc + 1, t);
+    }
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < E; ++v) xbuf[tid + T * v] = make_float2(x[v].x, -x[v].y);   // range index j
@@ -575,7 +578,8 @@ struct AfCrossArgs {
     const int16_t *tabq;    // float sinc table (Q15 taps, [phase][kTabRow])
     const float2 *tw;       // cross twiddles (m2)
     float *dacc;            // [mpad] per-slot Im sum conj(g_p1) p1
-    int m, n, mpad, window;
+    const double *acc;      // [0] sum |y1|^2, [1] sum I log I (complete once the range adjoint has run)
+    int m, n, mpad, window, n2;
 };
 
 // Shared-memory positions of bracket k and of W . F^H g at cross index k in the cross adjoint.  Its
@@ -625,13 +629,55 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
     }
     F::run(x, xbuf, a.tw, tid);
     const double hn = a.window ? a.ham_n[j] : 1.0;
+    // the -(E/S) z part of g_z: -(E/S) n2 m2 W^2 . R2 p1 at cross index k, R2 p1 from the forward brackets
+    const double S = a.acc[0] * (double)a.n2;
+    const double Ent = log(S) - a.acc[1] / S;
+    const float beta = (float)(-(Ent / S) * (double)a.n2 * (double)N);
+    const float2 *p1row = a.p1 + (size_t)j * a.mpad;
+    auto nat = [&](int t) { return asc ? t : m - 1 - t; };   // ascending-view source -> natural slot
     __syncthreads();
+    // four cross indices at a time: their two lerp samples are loaded (clamped indices, so unconditionally)
+    // before any is used, so the loads of the four overlap
+    constexpr int QB = E >= 4 ? 4 : E;
+    static_assert(E % QB == 0, "tile of whole load batches");
 #pragma unroll
-    for (int v = 0; v < E; ++v) {
-        const int k = tid + T * v;
-        float w = 0.f;
-        if (k < m) w = a.window ? (float)(a.ham_m[k] * hn) : 1.0f;
-        xbuf[y_at(k)] = make_float2(w * x[v].x, -w * x[v].y);   // W . F_cross^H g, cross index k
+    for (int v0 = 0; v0 < E; v0 += QB) {
+        uint32_t bb[QB];
+        float2 s0[QB], s1[QB];
+#pragma unroll
+        for (int c = 0; c < QB; ++c) {
+            const int k = tid + T * (v0 + c);
+            bb[c] = k < m ? pk[pk_at(k)] : 0x80000000u;
+            const int l = min(br_low(bb[c]), m - 2);
+            s0[c] = __ldg(p1row + nat(l));
+            s1[c] = __ldg(p1row + nat(l + 1));
+        }
+#pragma unroll
+        for (int c = 0; c < QB; ++c) {
+            const int v = v0 + c;
+            const int k = tid + T * v;
+            const float w = k < m ? (a.window ? (float)(a.ham_m[k] * hn) : 1.0f) : 0.f;
+            float2 fw = make_float2(0.f, 0.f);          // (R2 p1)[k]
+            if (!(bb[c] >> 31)) {
+                const int l = br_low(bb[c]);
+                if (SINC && l >= 15 && l <= m - 17) {
+                    const int16_t *ct = tab + (bb[c] & 0xffu) * kTabRow;
+#pragma unroll 8
+                    for (int t = 0; t < 32; ++t) {
+                        const float cf = (float)ct[t] * (1.0f / 32768.f);
+                        const float2 pv = __ldg(p1row + nat(l - 15 + t));
+                        fw.x = fmaf(cf, pv.x, fw.x);
+                        fw.y = fmaf(cf, pv.y, fw.y);
+                    }
+                } else {
+                    const float f = br_w(bb[c]);
+                    fw = make_float2(fmaf(f, s1[c].x - s0[c].x, s0[c].x), fmaf(f, s1[c].y - s0[c].y, s0[c].y));
+                }
+            }
+            const float bw = beta * w * w;
+            // W . F_cross^H g, cross index k
+            xbuf[y_at(k)] = make_float2(fmaf(bw, fw.x, w * x[v].x), fmaf(bw, fw.y, -w * x[v].y));
+        }
     }
     __syncthreads();
     const int r_lo = tid * E;
@@ -678,7 +724,6 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
 #pragma unroll
     for (int s2 = 0; s2 < E; ++s2) xbuf[F::pad(r_lo + s2)] = gs[s2];
     __syncthreads();
-    const float2 *p1row = a.p1 + (size_t)j * a.mpad;
     float2 pv[E];
 #pragma unroll
     for (int v = 0; v < E; ++v) {
@@ -695,10 +740,14 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
     }
 }
 
-__global__ void k_af_finish(const float *dacc, const int32_t *order, const double *acc, float *dtheta, double *ent, int m) {
+__global__ void k_af_finish(const float *dacc, const int32_t *order, const double *acc, float *dtheta, double *ent, int m,
+                            int n2) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r < m && dtheta) dtheta[order[r]] = 2.0f * dacc[r];
-    if (r == 0 && ent) ent[0] = log(acc[0]) - acc[1] / acc[0];
+    if (r == 0 && ent) {
+        const double S = acc[0] * (double)n2;
+        ent[0] = log(S) - acc[1] / S;
+    }
 }
 
 // One step of the autofocus descent on the device: g = dE/dtheta (2 dacc in slot order), theta <- theta -
@@ -761,8 +810,10 @@ cudaError_t launch_pass2(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, E>;
     FPass2Args p{d.p1_map, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabq, d.twm, d.y1, d.pk_out, d.wait_err,
                  d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0,
-                 d.mixed ? 0 : d.mx_probe};
-    const size_t sm = pass2_region_a(d.m, F::xbuf_elems()) + (SINC ? kTabShorts * 2 : 0) + 16;   // + 2 mbarriers
+                 d.mixed ? 0 : d.mx_probe, d.pk_out ? d.af_acc : nullptr};
+    // + 2 mbarriers + the autofocus forward's reduction scratch
+    const size_t sm = pass2_region_a(d.m, F::xbuf_elems()) + (SINC ? kTabShorts * 2 : 0) + 16 +
+                      (d.pk_out ? (size_t)8 * std::max(1, F::T / 32) : 0);
     auto fn = k_fl_pass2_fft<L, E, SINC>;
     if (d.pk_out) fn = k_fl_pass2_fft<L, E, SINC, true>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -931,13 +982,9 @@ cudaError_t launch_af_range(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, Cfg<L>::E>;
     AfRangeArgs p{d.y1, d.twn, d.af_acc, d.af_zadj, d.n, d.npad, d.m2};
     const size_t sm = (size_t)8 * F::xbuf_elems();
-    auto f1 = k_af_entropy<L, Cfg<L>::E>;
     auto f2 = k_af_range_adjoint<L, Cfg<L>::E>;
-    cudaError_t e = cudaFuncSetAttribute(f1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const cudaError_t e = cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    f1<<<d.m2, Cfg<L>::T, sm, st>>>(p);
     f2<<<d.m2, Cfg<L>::T, sm, st>>>(p);
     return cudaGetLastError();
 }
@@ -945,8 +992,8 @@ cudaError_t launch_af_range(const FloatDev &d, cudaStream_t st) {
 template <int L>
 cudaError_t launch_af_cross(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, Cfg<L>::E>;
-    AfCrossArgs p{d.af_zadj, d.p1, d.af_pk, d.ham_m64, d.ham_n64, d.kr, d.tan_s, d.tabq, d.twm, d.af_dacc,
-                  d.m, d.n, d.mpad, d.window};
+    AfCrossArgs p{d.af_zadj, d.p1, d.af_pk, d.ham_m64, d.ham_n64, d.kr, d.tan_s, d.tabq, d.twm, d.af_dacc, d.af_acc,
+                  d.m, d.n, d.mpad, d.window, d.n2};
     // exchange buffer, packed brackets (whole groups of 16), sinc table
     const size_t sm = (size_t)8 * F::xbuf_elems() + (size_t)4 * ((d.m + 15) & ~15) + (d.az_sinc ? kTabShorts * 2 : 0);
     auto fn = d.az_sinc ? k_af_cross_adjoint<L, Cfg<L>::E, true> : k_af_cross_adjoint<L, Cfg<L>::E, false>;
@@ -1017,7 +1064,7 @@ cudaError_t autofocus_grad(const FloatDev &d0, const float2 *sig, const float *t
     if ((e = pf.mark(st, "range_entropy_adjoint")) != cudaSuccess) return e;
     if ((e = af_cross(d, st)) != cudaSuccess) return e;
     if ((e = pf.mark(st, "cross_adjoint_pass2T")) != cudaSuccess) return e;
-    k_af_finish<<<(d.m + 255) / 256, 256, 0, st>>>(d.af_dacc, d.order, d.af_acc, dtheta, ent, d.m);
+    k_af_finish<<<(d.m + 255) / 256, 256, 0, st>>>(d.af_dacc, d.order, d.af_acc, dtheta, ent, d.m, d.n2);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return pf.mark(st, "finish");
 }
