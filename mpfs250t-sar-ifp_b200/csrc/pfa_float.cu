@@ -685,7 +685,27 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
 #pragma unroll
     for (int s2 = 0; s2 < E; ++s2) gs[s2] = make_float2(0.f, 0.f);
     if (r_lo < m) {
-        int lo = 0, hi = m;                             // first k with lower index >= r_lo - REACH_LO
+        // The brackets of queries outside the row's source span carry no weight.  They are a prefix of k
+        // (packed with lower index 0) and a suffix (lower index m - 2), so they sit inside the runs of
+        // the first and the last slots; walking them would cost those threads (and their CTA) one step per
+        // dead bracket and slot.  The walks cover only the live range [k0, k1).
+        int k0, k1;
+        {
+            int lo = 0, hi = m;                         // first k past the dead prefix
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                const uint32_t b = pk[pk_at(mid)];
+                if ((b >> 31) && br_low(b) == 0) lo = mid + 1; else hi = mid;
+            }
+            k0 = lo;
+            hi = m;                                     // first dead k at or after k0: the dead suffix
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (!(pk[pk_at(mid)] >> 31)) lo = mid + 1; else hi = mid;
+            }
+            k1 = lo;
+        }
+        int lo = k0, hi = k1;                           // first live k with lower index >= r_lo - REACH_LO
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
             if (br_low(pk[pk_at(mid)]) < r_lo - REACH_LO) lo = mid + 1; else hi = mid;
@@ -696,7 +716,7 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
             const int r = r_lo + s2;
             if (r < m) {
                 float2 gsum = make_float2(0.f, 0.f);
-                for (int kk = kp; kk < m; ++kk) {
+                for (int kk = kp; kk < k1; ++kk) {
                     const uint32_t b = pk[pk_at(kk)];
                     const int l = br_low(b);
                     if (l > r + REACH_HI) break;
@@ -713,7 +733,7 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
                     gsum.x = fmaf(wgt, y.x, gsum.x);
                     gsum.y = fmaf(wgt, y.y, gsum.y);
                 }
-                while (kp < m && br_low(pk[pk_at(kp)]) < r + 1 - REACH_LO) ++kp;
+                while (kp < k1 && br_low(pk[pk_at(kp)]) < r + 1 - REACH_LO) ++kp;
                 gs[s2] = gsum;
             }
         }
