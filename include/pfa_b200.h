@@ -202,10 +202,12 @@ pfa_status pfa_form_float_host(pfa_plan *plan, const float *sig_host, void *out_
  * natural layout), its
  * entropy E = -sum p log p with p = |z|^2 / sum |z|^2, and dE/dtheta[m] with hand-written adjoint
  * kernels (range FFT recomputed, adjoint FFTs, window, transposed pass-2 resample -- lerp or 32-tap sinc --
- * as an atomics-free segmented reduction; descending source axes included).  entropy_dev (double, device) may be NULL.  The first call on a plan adds its
- * gradient workspace to the plan (12 n pow2(m) bytes at most: the range-FFT adjoint and the packed
- * pass-2 brackets), held until pfa_plan_destroy and not counted by pfa_plan_workspace_bytes.  The
- * reference has no autofocus; the image it forms is form_image_pfa.pfa (src/form_image_pfa.py:243-246). */
+ * as an atomics-free segmented reduction; descending source axes included).  entropy_dev (double,
+ * device) may be NULL.  The first call on a plan adds its gradient workspace to the plan (12 n pow2(m)
+ * bytes at most: the range-FFT adjoint and the packed pass-2 brackets; a float-sinc plan adds 8 n m
+ * bytes for the forward's resampled rows), held until pfa_plan_destroy and not counted by
+ * pfa_plan_workspace_bytes.  The reference has no autofocus; the image it forms is form_image_pfa.pfa
+ * (src/form_image_pfa.py:243-246). */
 pfa_status pfa_autofocus_grad(pfa_plan *plan, const float *sig_dev, const float *theta_dev, float *dtheta_dev,
                               double *entropy_dev, void *stream);
 

@@ -252,7 +252,9 @@ struct FPass2Args {
     const int16_t *tabq;
     const float2 *tw;
     float2 *y1t;          // [m2][npad] cross-FFT output, transposed: row = cross bin, col = range bin
-    uint32_t *pk_out;     // lerp: packed brackets [j][k] for the autofocus adjoint, or nullptr
+    uint32_t *pk_out;     // packed brackets [j][k] for the autofocus adjoint, or nullptr
+    float2 *rp_out;       // float sinc, autofocus forward: R2 p1 [j][k] before the window (the adjoint's
+                          // W^2 R2 p1 term), or nullptr
     int *err;             // set when the row load's bounded wait runs out
     int m, n, mpad, npad, centred, window, inverse;
     int probe;            // test hook: > 0 = first wait this many polls on a barrier nothing arrives on
@@ -385,11 +387,14 @@ k_fl_pass2_fft(const __grid_constant__ FPass2Args a) {
                 const int lowi = bl[u] & 0xffff;
                 const Frac fr{bf[u], (bl[u] >> 16) & 0xff, (bl[u] >> 24) & 1};
                 val = gather_f32<SINC>(row, 0, m, lowi, fr, tab);
+                if constexpr (PK && SINC) a.rp_out[(size_t)j * m + k] = val;   // R2 p1 for the adjoint
                 // np.outer(hamming(m), hamming(n)).astype(float32)[k, j]
                 const float wgt = a.window ? (float)(a.ham_m[k] * hn) : 1.0f;
                 const float sg = (a.centred && ((j + k) & 1)) ? -wgt : wgt;
                 val.x *= sg;
                 val.y *= sg;
+            } else if constexpr (PK && SINC) {
+                a.rp_out[(size_t)j * m + k] = make_float2(0.f, 0.f);
             }
         }
         x[u] = a.inverse ? make_float2(val.x, -val.y) : val;
@@ -573,6 +578,7 @@ struct AfCrossArgs {
     const float2 *zadj_t;   // [n][m2]
     const float2 *p1;       // [n][mpad] forward pass-1 output (phase corrected)
     const uint32_t *pk;     // [n][m] packed brackets of the forward pass 2 (ascending view)
+    const float2 *rp;       // [n][m] float sinc: R2 p1 of the forward pass 2 (before the window)
     const double *ham_m, *ham_n;
     const double *kr_grid, *tan_s;   // the direction of range bin j's pass-2 source axis
     const int16_t *tabq;    // float sinc table (Q15 taps, [phase][kTabRow])
@@ -648,9 +654,14 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
         for (int c = 0; c < QB; ++c) {
             const int k = tid + T * (v0 + c);
             bb[c] = k < m ? pk[pk_at(k)] : 0x80000000u;
-            const int l = min(br_low(bb[c]), m - 2);
-            s0[c] = __ldg(p1row + nat(l));
-            s1[c] = __ldg(p1row + nat(l + 1));
+            if constexpr (SINC) {
+                // the forward pass 2 stored R2 p1 (its 32-tap gathers): one coalesced load per cross index
+                s0[c] = k < m ? __ldcs(a.rp + (size_t)j * m + k) : make_float2(0.f, 0.f);
+            } else {
+                const int l = min(br_low(bb[c]), m - 2);
+                s0[c] = __ldg(p1row + nat(l));
+                s1[c] = __ldg(p1row + nat(l + 1));
+            }
         }
 #pragma unroll
         for (int c = 0; c < QB; ++c) {
@@ -658,21 +669,11 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
             const int k = tid + T * v;
             const float w = k < m ? (a.window ? (float)(a.ham_m[k] * hn) : 1.0f) : 0.f;
             float2 fw = make_float2(0.f, 0.f);          // (R2 p1)[k]
-            if (!(bb[c] >> 31)) {
-                const int l = br_low(bb[c]);
-                if (SINC && l >= 15 && l <= m - 17) {
-                    const int16_t *ct = tab + (bb[c] & 0xffu) * kTabRow;
-#pragma unroll 8
-                    for (int t = 0; t < 32; ++t) {
-                        const float cf = (float)ct[t] * (1.0f / 32768.f);
-                        const float2 pv = __ldg(p1row + nat(l - 15 + t));
-                        fw.x = fmaf(cf, pv.x, fw.x);
-                        fw.y = fmaf(cf, pv.y, fw.y);
-                    }
-                } else {
-                    const float f = br_w(bb[c]);
-                    fw = make_float2(fmaf(f, s1[c].x - s0[c].x, s0[c].x), fmaf(f, s1[c].y - s0[c].y, s0[c].y));
-                }
+            if constexpr (SINC) {
+                fw = s0[c];
+            } else if (!(bb[c] >> 31)) {
+                const float f = br_w(bb[c]);
+                fw = make_float2(fmaf(f, s1[c].x - s0[c].x, s0[c].x), fmaf(f, s1[c].y - s0[c].y, s0[c].y));
             }
             const float bw = beta * w * w;
             // W . F_cross^H g, cross index k
@@ -828,7 +829,7 @@ struct Cfg {
 template <int L, int E, bool SINC>
 cudaError_t launch_pass2(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, E>;
-    FPass2Args p{d.p1_map, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabq, d.twm, d.y1, d.pk_out, d.wait_err,
+    FPass2Args p{d.p1_map, d.tan_s, d.kr, d.kc, d.ham_m64, d.ham_n64, d.tabq, d.twm, d.y1, d.pk_out, d.rp_out, d.wait_err,
                  d.m, d.n, d.mpad, d.npad, d.layout == PFA_LAYOUT_CENTRED, d.window, d.sgn > 0,
                  d.mixed ? 0 : d.mx_probe, d.pk_out ? d.af_acc : nullptr};
     // + 2 mbarriers + the autofocus forward's reduction scratch
@@ -961,7 +962,7 @@ cudaError_t float_alloc(FloatDev &d, int m, int n) {
 void float_free(FloatDev &d) {
     dfr(d.f0); dfr(d.df); dfr(d.flast); dfr(d.pr); dfr(d.tan_s); dfr(d.order); dfr(d.kr); dfr(d.kc); dfr(d.ham_m64);
     dfr(d.ham_n64); dfr(d.twm); dfr(d.twn); dfr(d.tabq); dfr(d.p1); dfr(d.y1); dfr(d.wait_err);
-    dfr(d.af_zadj); dfr(d.af_acc); dfr(d.af_dacc); dfr(d.af_pk);
+    dfr(d.af_zadj); dfr(d.af_acc); dfr(d.af_dacc); dfr(d.af_pk); dfr(d.af_rp);
     mixed_free(d);
 }
 
@@ -1012,7 +1013,7 @@ cudaError_t launch_af_range(const FloatDev &d, cudaStream_t st) {
 template <int L>
 cudaError_t launch_af_cross(const FloatDev &d, cudaStream_t st) {
     using F = F32Fft<L, Cfg<L>::E>;
-    AfCrossArgs p{d.af_zadj, d.p1, d.af_pk, d.ham_m64, d.ham_n64, d.kr, d.tan_s, d.tabq, d.twm, d.af_dacc, d.af_acc,
+    AfCrossArgs p{d.af_zadj, d.p1, d.af_pk, d.af_rp, d.ham_m64, d.ham_n64, d.kr, d.tan_s, d.tabq, d.twm, d.af_dacc, d.af_acc,
                   d.m, d.n, d.mpad, d.window, d.n2};
     // exchange buffer, packed brackets (whole groups of 16), sinc table
     const size_t sm = (size_t)8 * F::xbuf_elems() + (size_t)4 * ((d.m + 15) & ~15) + (d.az_sinc ? kTabShorts * 2 : 0);
@@ -1067,6 +1068,7 @@ cudaError_t autofocus_grad(const FloatDev &d0, const float2 *sig, const float *t
     d.layout = PFA_LAYOUT_NATURAL;      // |z| (so E) does not depend on the centring
     d.sgn = -1;
     d.pk_out = d.af_pk;                 // the forward pass 2 keeps its brackets for the cross adjoint
+    d.rp_out = d.az_sinc ? d.af_rp : nullptr;   // and, float sinc, its resampled rows
     if ((e = cudaMemsetAsync(d.af_acc, 0, 2 * sizeof(double), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(d.af_dacc, 0, sizeof(float) * d.mpad, st)) != cudaSuccess) return e;
     FPass1Args p1{sig, d.f0, d.df, d.flast, d.pr, d.kr, d.order, d.tabq, theta, d.p1, d.m, d.n, d.mpad};
@@ -1274,8 +1276,9 @@ static pfa_status autofocus_common(pfa_plan *p, const float *sig_dev, const floa
     if (!d.af_zadj) {
         if ((e = pfa::dal(&d.af_zadj, (size_t)d.n * d.m2)) != cudaSuccess ||
             (e = pfa::dal(&d.af_acc, 2)) != cudaSuccess || (e = pfa::dal(&d.af_dacc, d.mpad)) != cudaSuccess ||
-            (e = pfa::dal(&d.af_pk, (size_t)d.n * d.m)) != cudaSuccess) {
-            pfa::dfr(d.af_zadj); pfa::dfr(d.af_acc); pfa::dfr(d.af_dacc); pfa::dfr(d.af_pk);
+            (e = pfa::dal(&d.af_pk, (size_t)d.n * d.m)) != cudaSuccess ||
+            (d.az_sinc && (e = pfa::dal(&d.af_rp, (size_t)d.n * d.m)) != cudaSuccess)) {
+            pfa::dfr(d.af_zadj); pfa::dfr(d.af_acc); pfa::dfr(d.af_dacc); pfa::dfr(d.af_pk); pfa::dfr(d.af_rp);
             return fcuda(p, e, "autofocus workspace");
         }
     }

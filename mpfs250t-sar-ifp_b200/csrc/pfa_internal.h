@@ -57,6 +57,8 @@ struct FloatDev {
     float *af_dacc = nullptr;          // [mpad] per-slot gradient accumulators
     uint32_t *af_pk = nullptr;         // [n][m] autofocus: packed pass-2 brackets of the forward pass
     uint32_t *pk_out = nullptr;        // where pass 2 stores its packed brackets for the adjoint (or nullptr)
+    float2 *af_rp = nullptr;           // [n][m] autofocus, float-sinc plans: the forward's resampled rows R2 p1
+    float2 *rp_out = nullptr;          // where a float-sinc pass 2 stores R2 p1 for the adjoint (or nullptr)
     // split-precision (mixed) mode: tensor-core FFTs for lines of 2048..8192 points
     int mixed = 0;
     uint4 *mx_f128 = nullptr;          // F_128 TMEM image [128 lanes][256 columns] of fp16 pairs
