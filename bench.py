@@ -332,6 +332,17 @@ def measure_modes(a, local):
                              "entropy_true_phase": round(float(e_true), 5),
                              "phase_rms_rad_before_after_50_steps": [round(float(np.sqrt(np.mean(res0 ** 2))), 4),
                                                                      round(float(np.sqrt(np.mean(res ** 2))), 4)]}
+    # the same gradient through the float 32-tap sinc passes (transposed sinc resample in the adjoint)
+    with engine.FloatPlan(4096, 4096, True, True, device=local) as plan:
+        plan.set_tables(tables)
+        theta = torch.zeros(4096, dtype=torch.float32, device=sig.device)
+        ms_s = _device_ms(lambda: autofocus.entropy_grad(plan, sig, theta, dth, ent), steps, 3)
+        plan.set_profiling(True)
+        autofocus.entropy_grad(plan, sig, theta, dth, ent)
+        st_s = plan.stage_times()
+        plan.set_profiling(False)
+    out["autofocus_4096"]["sinc"] = {"ms_per_grad": round(ms_s, 4), "grads_per_s": round(1000.0 / ms_s, 1),
+                                     "stages_ms": {k: round(v, 4) for k, v in st_s.items()}}
     del sig
     out["batch_16_uneven"] = measure_batch(a, local)
     return out

@@ -712,6 +712,52 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
             if (br_low(pk[pk_at(mid)]) < r_lo - REACH_LO) lo = mid + 1; else hi = mid;
         }
         int kp = lo;
+        if constexpr (SINC) {
+            // Bracket-outer: every live bracket whose taps reach one of this thread's E slots (lower index
+            // l in [r_lo - 16, r_lo + E + 14]) is read once and added to each slot it reaches, in the same
+            // increasing-k order per slot as a slot-by-slot walk.  Interior brackets add tap r - l + 15 of
+            // their phase row as the integer Q15 value, edge brackets their lerp weights times 2^15; the
+            // sums are scaled by 2^-15 at the end (a power of two commutes with every rounding, so each sum
+            // is the one the float taps give).
+            for (int kk = kp; kk < k1; ++kk) {
+                const uint32_t b = pk[pk_at(kk)];
+                const int l = br_low(b);
+                if (l > r_lo + E - 1 + REACH_HI) break;
+                const float2 y = xbuf[y_at(kk)];
+                if (l >= 15 && l <= m - 17) {
+                    const int16_t *row = tab + (b & 0xffu) * kTabRow;
+                    const int t0 = r_lo - l + 15;          // tap of slot r_lo
+#pragma unroll
+                    for (int s2 = 0; s2 < E; ++s2) {
+                        if ((unsigned)(t0 + s2) < 32u) {
+                            const float w = s16f(row[t0 + s2]);
+                            gs[s2].x = fmaf(w, y.x, gs[s2].x);
+                            gs[s2].y = fmaf(w, y.y, gs[s2].y);
+                        }
+                    }
+                } else if (!(b >> 31)) {
+                    const float f = br_w(b);
+                    const float w0 = (1.0f - f) * 32768.f, w1 = f * 32768.f;
+#pragma unroll
+                    for (int s2 = 0; s2 < E; ++s2) {
+                        const int r = r_lo + s2;
+                        if (r == l) {
+                            gs[s2].x = fmaf(w0, y.x, gs[s2].x);
+                            gs[s2].y = fmaf(w0, y.y, gs[s2].y);
+                        } else if (r == l + 1) {
+                            gs[s2].x = fmaf(w1, y.x, gs[s2].x);
+                            gs[s2].y = fmaf(w1, y.y, gs[s2].y);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int s2 = 0; s2 < E; ++s2) {
+                gs[s2].x *= 1.0f / 32768.f;
+                gs[s2].y *= 1.0f / 32768.f;
+                if (r_lo + s2 >= m) gs[s2] = make_float2(0.f, 0.f);
+            }
+        } else {
 #pragma unroll
         for (int s2 = 0; s2 < E; ++s2) {
             const int r = r_lo + s2;
@@ -737,6 +783,7 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
                 while (kp < k1 && br_low(pk[pk_at(kp)]) < r + 1 - REACH_LO) ++kp;
                 gs[s2] = gsum;
             }
+        }
         }
     }
     // the slot sums go through shared memory (padded: a thread's E consecutive slots hit distinct banks)
