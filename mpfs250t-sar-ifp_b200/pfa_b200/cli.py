@@ -8,7 +8,8 @@ The input is a seeded synthetic scene of the given shape (or ``--input`` a compl
 with ``--tables`` an .npz of ``prepare_tables`` output).  Prints the device time of every frame; ``--out``
 saves the last image.  Modes: ``fixed`` (bit-exact emulator datapath), ``float`` (FP32), ``mixed``
 (split-precision tensor-core FFTs) and ``autofocus`` (the image-entropy gradient w.r.t. the per-pulse
-phase of a scene with the injected quadratic + random-walk phase error; one gradient per frame).
+phase of a scene with the injected quadratic + random-walk phase error; one gradient per frame, through
+the float-sinc passes with ``--range-sinc`` / ``--az-sinc``).
 ``--display`` adds the device display scaling of save_detected_geotiff to each float frame.
 """
 from __future__ import annotations
@@ -58,7 +59,7 @@ def main(argv=None) -> int:
         phi = torch.as_tensor(synth.phase_error(m, seed=a.seed), device=dev)
         sig = (sig * torch.polar(torch.ones_like(phi), phi)[:, None].to(torch.complex64)).contiguous()
         theta = torch.zeros(m, dtype=torch.float32, device=dev)
-        with engine.FloatPlan(m, n, device=a.device) as plan:
+        with engine.FloatPlan(m, n, a.range_sinc, a.az_sinc, device=a.device) as plan:
             plan.set_tables(tb)
             for k in range(a.frames):
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -66,7 +67,8 @@ def main(argv=None) -> int:
                 ent, dth = autofocus.entropy_grad(plan, sig, theta)
                 e1.record()
                 torch.cuda.synchronize()
-                print(f"gradient {k}: {e0.elapsed_time(e1):.3f} ms  (entropy {float(ent):.5f}, {m}x{n})")
+                print(f"gradient {k}: {e0.elapsed_time(e1):.3f} ms  (entropy {float(ent):.5f}, {m}x{n}"
+                      f"{', sinc' if a.range_sinc or a.az_sinc else ''})")
         return 0
     if a.mode == "fixed":
         grid = a.grid or geometry.pow2(max(m, n))
