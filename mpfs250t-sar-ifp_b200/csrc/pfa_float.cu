@@ -599,9 +599,10 @@ __device__ __forceinline__ float br_w(uint32_t p) { return (float)(p & 0x1ffffu)
 // R2^H as an atomics-free segmented reduction.  On the ascending view of the sources, bracket k (lower index
 // l_k, monotone in k) touches slots l_k and l_k + 1 (lerp: weights 1 - f and f) or, for an interior float
 // sinc bracket, slots l_k - 15 .. l_k + 16 (weight tab[phase][u - l_k + 15] / 2^15).  So slot u collects
-// the contiguous run of k with l_k in [u - 16, u + 15] (sinc) or [u - 1, u] (lerp), and each thread walks
-// one run for its E consecutive slots.  A descending source axis maps ascending slot u to natural slot
-// m - 1 - u (the forward mirrors the bracket and reverses the taps, which is the same linear map).
+// the contiguous run of k with l_k in [u - 16, u + 15] (sinc) or [u - 1, u] (lerp).  Each thread owns E
+// consecutive slots: the lerp walks one run per slot; the sinc reads each bracket of the union of its
+// slots' runs once and adds it to every slot it reaches.  A descending source axis maps ascending slot u to
+// natural slot m - 1 - u (the forward mirrors the bracket and reverses the taps, which is the same map).
 template <int L, int E, bool SINC>
 __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_adjoint(AfCrossArgs a) {
     using F = F32Fft<L, E>;
@@ -759,31 +760,25 @@ __global__ void __launch_bounds__((1 << L) / E, fl_min_ctas(L, E)) k_af_cross_ad
             }
         } else {
 #pragma unroll
-        for (int s2 = 0; s2 < E; ++s2) {
-            const int r = r_lo + s2;
-            if (r < m) {
-                float2 gsum = make_float2(0.f, 0.f);
-                for (int kk = kp; kk < k1; ++kk) {
-                    const uint32_t b = pk[pk_at(kk)];
-                    const int l = br_low(b);
-                    if (l > r + REACH_HI) break;
-                    if (b >> 31) continue;
-                    float wgt;
-                    if (SINC && l >= 15 && l <= m - 17) {
-                        const int t = r - l + 15;
-                        wgt = (t >= 0 && t < 32) ? (float)tab[(b & 0xffu) * kTabRow + t] * (1.0f / 32768.f) : 0.f;
-                    } else {
+            for (int s2 = 0; s2 < E; ++s2) {
+                const int r = r_lo + s2;
+                if (r < m) {
+                    float2 gsum = make_float2(0.f, 0.f);
+                    for (int kk = kp; kk < k1; ++kk) {
+                        const uint32_t b = pk[pk_at(kk)];
+                        const int l = br_low(b);
+                        if (l > r + REACH_HI) break;
+                        if (b >> 31) continue;
                         const float f = br_w(b);
-                        wgt = (l == r) ? 1.0f - f : (l == r - 1 ? f : 0.f);
+                        const float wgt = (l == r) ? 1.0f - f : (l == r - 1 ? f : 0.f);
+                        const float2 y = xbuf[y_at(kk)];
+                        gsum.x = fmaf(wgt, y.x, gsum.x);
+                        gsum.y = fmaf(wgt, y.y, gsum.y);
                     }
-                    const float2 y = xbuf[y_at(kk)];
-                    gsum.x = fmaf(wgt, y.x, gsum.x);
-                    gsum.y = fmaf(wgt, y.y, gsum.y);
+                    while (kp < k1 && br_low(pk[pk_at(kp)]) < r + 1 - REACH_LO) ++kp;
+                    gs[s2] = gsum;
                 }
-                while (kp < k1 && br_low(pk[pk_at(kp)]) < r + 1 - REACH_LO) ++kp;
-                gs[s2] = gsum;
             }
-        }
         }
     }
     // the slot sums go through shared memory (padded: a thread's E consecutive slots hit distinct banks)
