@@ -759,7 +759,9 @@ __global__ void __launch_bounds__(256) k_fx_detect(const uint32_t *__restrict__ 
                                                    const int32_t *__restrict__ ctrl, uint16_t *__restrict__ img, int G,
                                                    int fused) {
     __shared__ uint16_t t[128][65];
-    const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 128;
+    // k tiles in reverse: FFT-2 wrote its rows in increasing k just before, so the first tiles read the
+    // rows most likely still in L2
+    const int k0 = (gridDim.y - 1 - blockIdx.y) * 64, j0 = blockIdx.x * 128;
     const int emax2 = ctrl[2];
     const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;   // 64 column pairs x 4 rows
     // all 16 loads of this thread in flight before any arithmetic
