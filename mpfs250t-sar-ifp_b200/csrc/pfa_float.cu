@@ -298,7 +298,9 @@ k_fl_pass2_fft(const __grid_constant__ FPass2Args a) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     const int tid = threadIdx.x;
-    const int j = blockIdx.x;
+    // clusters in reverse range-bin order (a cluster's CTAs stay adjacent, rank order kept): pass 1 wrote
+    // the high range-bin rows of p1 last, so the first clusters find their rows in L2
+    const int j = (int)(gridDim.x - kCT - (blockIdx.x & ~(kCT - 1)) + (blockIdx.x & (kCT - 1)));
     const bool live = j < a.n;                 // grid is padded to a multiple of the cluster size
     float2 x[E];
     bool landed = true, issued = false;
